@@ -1,0 +1,382 @@
+"""Benchmark of the moment-encoded LBM fluid step on B200.
+
+Default workload (one GPU): D3Q27 384x192x192 channel with an undulating
+ellipsoid swimmer (~4k vertices, 8k triangles), FP32 moment storage: one
+step = link detection + fused stream/reconstruct/collide/re-encode pass +
+moving-wall links with surface forces + outlet update.  Metric: MLUPS
+(million lattice-cell updates per second, whole job), with the dense kernel's
+fraction of the measured HBM peak.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload D|C|B|A] [--storage f32|f16|bf16] [--small]
+
+N > 1 runs one independent replica per GPU (the single-grid path has no
+exchange step; see DESIGN.md "multi-GPU"), launched by torchrun; the time is
+the max over ranks and value = all cells updated / that time ("weak").
+
+``--impl reference`` times the reference's algorithm on the host cores: the
+FP32 restatement in oracle/ (the reference's CUDA sources do not build here)
+with all host threads, each step a z-slab sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from freeflow_b200 import workloads as W  # noqa: E402
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def algorithmic_bytes_per_cell(dim: int, storage: str) -> int:
+    """2 * NM * s + 1: read and write NM moments of s bytes, read one flag byte."""
+    nm = 6 if dim == 2 else 10
+    s = 4 if storage == "f32" else 2
+    return 2 * nm * s + 1
+
+
+def make_workload(name: str, small: bool):
+    if name == "D":
+        return W.swimmer_3d(nx=256, ny=128, nz=128) if small else W.swimmer_3d()
+    if name == "C":
+        return W.taylor_green_3d(n=96 if small else 128)
+    if name == "B":
+        return W.swimmer_2d(nx=600, ny=200) if small else W.swimmer_2d()
+    if name == "A":
+        return W.cylinder_channel_2d()
+    raise ValueError(name)
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU (oracle)
+def oracle_slab_run(wl: W.Workload, steps: int, warmup: int, nz_slab: int, threads: int, precision="ref32"):
+    """Time the oracle on a z-slab of the workload (3D) or the whole grid (2D).
+    Returns (MLUPS, cells per step, seconds)."""
+    from oracle import oracle as O
+
+    O.set_threads(threads)
+    if wl.dim == 3:
+        nz_slab = max(3, min(nz_slab, wl.nz))
+        z0 = max(0, wl.nz // 2 - nz_slab // 2)
+        nxy = wl.nx * wl.ny
+        flags = wl.flags[z0 * nxy:(z0 + nz_slab) * nxy]
+        mom = wl.moments[z0 * nxy:(z0 + nz_slab) * nxy]
+        shift = np.array([0.0, 0.0, z0 * wl.fluid_dx], dtype=np.float32)
+        nz = nz_slab
+    else:
+        flags, mom, shift, nz = wl.flags, wl.moments, None, 1
+    o = O.Oracle(wl.dim, wl.nx, wl.ny, nz, viscosity=wl.fluid_viscosity, density=wl.fluid_density,
+                 dx=wl.fluid_dx, dt=wl.dt, boundary_velocities=wl.boundary_velocities, periodic=wl.periodic,
+                 precision=precision)
+    o.set_flags(flags)
+    o.set_moments(mom.astype(np.float64))
+    F = np.zeros(wl.rest.size, dtype=np.float64) if wl.elements is not None else None
+
+    def one(s):
+        if wl.elements is None:
+            o.step()
+            return
+        v, u = wl.surface_at(s)
+        if shift is not None:
+            v = v - shift
+        o.step(v, u, wl.elements, F)
+
+    for s in range(warmup):
+        one(s)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        one(warmup + s)
+    dt = time.perf_counter() - t0
+    cells = wl.nx * wl.ny * nz
+    return cells * steps / dt / 1e6, cells, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = make_workload(args.workload, args.small)
+    threads = os.cpu_count() or 1
+    # size the slab so that the whole (K + W)-step run stays near two minutes
+    rate = 4.0e6 * threads / 8.0  # cell updates / s, measured order of the oracle
+    budget_s = 120.0
+    nz_slab = int(budget_s * rate / max(1, args.steps + args.warmup) / (wl.nx * wl.ny))
+    mlups, cells, sec = oracle_slab_run(wl, args.steps, args.warmup, nz_slab, threads)
+    sample = (f"{'z-slab ' + str(cells // (wl.nx * wl.ny)) + ' of ' + str(wl.nz) + ' planes' if wl.dim == 3 else 'full grid'}"
+              f" of {wl.name} ({cells} cells per step), {args.steps} steps")
+    out = {
+        "metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * sec / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "impl": "reference",
+        "config": {"workload": wl.name, "cells": wl.ncell, "storage": "f32"},
+        "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------- GPU
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    from freeflow_b200 import DeviceSurface, FluidGrid
+
+    wl = make_workload(args.workload, args.small)
+    K, Wm = args.steps, args.warmup
+    storage = args.storage
+    g = FluidGrid(**wl.grid_kwargs(storage=storage))
+    g.set_flags(wl.flags)
+    g.set_moments(wl.moments)
+    stream = torch.cuda.Stream()
+    surf = None
+    nsteps_total = K + Wm
+    if wl.elements is not None:
+        v0, u0 = wl.surface_at(0)
+        surf = DeviceSurface(v0, u0, wl.elements)
+        g.reserve_surface(surf.num_vertices, max(4096, surf.num_elements * 40))
+        # per-step surfaces for the device-resident run
+        V = np.empty((nsteps_total,) + v0.shape, np.float32)
+        U = np.empty_like(V)
+        for s in range(nsteps_total):
+            V[s], U[s] = wl.surface_at(s)
+        Vd = torch.from_numpy(V).cuda()
+        Ud = torch.from_numpy(U).cuda()
+
+    def step(s):
+        if surf is not None:
+            surf.vertices = Vd[s]
+            surf.velocities = Ud[s]
+            g.step(surf, stream=stream)
+        else:
+            g.step(stream=stream)
+
+    with torch.cuda.stream(stream):
+        for s in range(Wm):
+            step(s)
+    torch.cuda.synchronize()
+    if g.status(clear=True):
+        print(json.dumps({"warning": "device status set during warm-up"}), file=sys.stderr)
+
+    # ---- timed region: inputs resident in HBM (both moment buffers exceed L2)
+    clocks = ClockSampler(torch.cuda.current_device())
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    g.profile(True)
+    g.profile_read(reset=True)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    with torch.cuda.stream(stream):
+        for s in range(K):
+            step(Wm + s)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    g.profile(False)
+    prof = g.profile_read(reset=True)
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    status = g.status(clear=True)
+
+    # ---- end to end: host surface in pinned memory -> step -> forces to host
+    e2e = None
+    if surf is not None:
+        Vh = torch.from_numpy(V).pin_memory()
+        Uh = torch.from_numpy(U).pin_memory()
+        Fh = torch.empty(surf.forces.shape, dtype=torch.float32).pin_memory()
+        vbuf = torch.empty_like(surf.forces)
+        ubuf = torch.empty_like(surf.forces)
+        surf.vertices, surf.velocities = vbuf, ubuf
+
+        def e2e_step(s):
+            vbuf.copy_(Vh[s], non_blocking=True)
+            ubuf.copy_(Uh[s], non_blocking=True)
+            surf.forces.zero_()
+            g.step(surf, stream=stream)
+            Fh.copy_(surf.forces, non_blocking=True)
+
+        with torch.cuda.stream(stream):
+            for s in range(Wm):
+                e2e_step(s)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            for s in range(K):
+                e2e_step(Wm + s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nb = surf.num_vertices * wl.dim * 4
+        e2e = {"value": round(world * wl.ncell * K / (ems * 1e-3) / 1e6, 1), "unit": "MLUPS",
+               "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb}
+    else:
+        # no surface: the step's inputs are the moments themselves; e2e = upload
+        # the initial state once, step, read back the density field once
+        e2e = None
+
+    value = world * wl.ncell * K / (ms * 1e-3) / 1e6
+    peak, peak_kind = hbm_peak()
+    bpc = algorithmic_bytes_per_cell(wl.dim, storage)
+    dense_ms, dense_n = prof["dense"]
+    dense_avg_s = dense_ms * 1e-3 / max(1, dense_n)
+    achieved = wl.ncell * bpc / dense_avg_s / 1e9
+    launches_per_step = 1 + (3 if surf is not None else 0)
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            rate = 4.0e6 * threads / 8.0
+            nz_slab = int(20.0 * rate / 3 / (wl.nx * wl.ny)) if wl.dim == 3 else 1
+            mlups, cells, sec = oracle_slab_run(wl, 3, 1, nz_slab, threads)
+            cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+                   "sample": (f"3 steps of a {cells // (wl.nx * wl.ny)}-plane z-slab of {wl.name}" if wl.dim == 3
+                              else f"3 steps of {wl.name}") + f", FP32 restatement, {sec:.1f} s"}
+        out = {
+            "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
+            "warmup": Wm, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": storage, "data": "synthetic (seeded)",
+            "config": {"workload": wl.name, "cells": wl.ncell, "storage": storage,
+                       "surface": (f"{surf.num_vertices} vertices / {surf.num_elements} elements" if surf else None),
+                       "l2": "moment buffers exceed L2 (no flush needed)" if wl.ncell * bpc > 2 * 126e6
+                       else "inputs smaller than L2", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "dense3d_kernel" if wl.dim == 3 else "dense2d_kernel",
+                         "bytes_per_cell": bpc, "kernel_ms": round(dense_ms / max(1, dense_n), 4)},
+            "stages_ms_per_step": {k: round(v[0] / max(1, v[1]), 4) for k, v in prof.items() if v[1]},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * K,
+            "clocks": clk,
+            "device_status": status,
+        }
+        print(json.dumps(out), flush=True)
+    g.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="D", choices=["A", "B", "C", "D"])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--small", action="store_true", help="reduced grid (profiling captures)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,197 @@
+// Grid set-up kernels: derived flag bits, initial state, solid fill and the
+// moment layout / precision conversions used by the C ABI.
+#include <algorithm>
+
+#include "ffs_common.cuh"
+#include "ffs_geom.cuh"
+#include "ffs_links.cuh"
+#include "ffs_outlet.cuh"
+
+namespace fflbm {
+
+namespace {
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+template <int DIM> __device__ __forceinline__ void dir3(int i, int &cx, int &cy, int &cz)
+{
+    cx = Lattice<DIM>::cx(i); cy = Lattice<DIM>::cy(i); cz = Lattice<DIM>::cz(i);
+}
+} // namespace
+
+// Per cell: the bounce-back mask (bit i set when the wrapped neighbour
+// x - c_i is a wall type, as the reference tests every step at
+// FsiCoupling2D.cu:159-176 / FsiCoupling3D.cu:199-216), NEAR_WALL when the
+// mask is non-zero, and OUTLET_SRC when the cell is the Fluid feeder of an
+// outlet node.  Node types are static between flag uploads, so this runs
+// once per upload instead of every step.
+template <int DIM>
+__global__ void prepare_flags_kernel(uint8_t *flags, uint32_t *wallmask, int nx, int ny, int nz)
+{
+    constexpr int Q = Lattice<DIM>::Q;
+    const long long nxy = (long long)nx * ny, n = nxy * nz;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / nxy);
+        const uint32_t t = flags[c] & kTypeMask;
+        uint32_t mask = 0;
+#pragma unroll
+        for (int i = 1; i < Q; ++i) {
+            int cx, cy, cz;
+            dir3<DIM>(i, cx, cy, cz);
+            long long ib = ((long long)wrapi(z - cz, nz) * ny + wrapi(y - cy, ny)) * nx + wrapi(x - cx, nx);
+            if (is_bounce_back<DIM>(flags[ib] & kTypeMask)) mask |= 1u << i;
+        }
+        uint8_t bits = (uint8_t)t;
+        if (mask) bits |= kBitNearWall;
+        if (t == kFluid) {
+            for (int r = 0; r < kNumOutletRules<DIM>; ++r) {
+                long long q = c + outlet_offset<DIM>(r, nx, nxy);
+                if (q >= 0 && q < n && (flags[q] & kTypeMask) == outlet_rule<DIM>(r).type) bits |= kBitOutletSrc;
+            }
+        }
+        wallmask[c] = mask;
+        flags[c] = bits; // neighbours only read the type bits, which do not change
+    }
+}
+
+template <int DIM>
+cudaError_t launch_prepare_flags(uint8_t *flags, uint32_t *wallmask, int nx, int ny, int nz, cudaStream_t st)
+{
+    long long n = (long long)nx * ny * nz;
+    int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    prepare_flags_kernel<DIM><<<grid, 256, 0, st>>>(flags, wallmask, nx, ny, nz);
+    return cudaGetLastError();
+}
+template cudaError_t launch_prepare_flags<2>(uint8_t *, uint32_t *, int, int, int, cudaStream_t);
+template cudaError_t launch_prepare_flags<3>(uint8_t *, uint32_t *, int, int, int, cudaStream_t);
+
+// initialize_state_kernel_2d/3d (LbmInitializer2D.cu:32-95,
+// LbmInitializer3D.cu:33-113): rho = 1, u set on inlet nodes from the
+// boundary velocities, equilibrium stress pi_ab = u_a u_b (the second moments
+// of the reference's second-order feq, evaluated exactly), both buffers.
+template <int DIM, typename T>
+__global__ void initialize_kernel(GridArgs<T> g, T *other, Vel6 bc)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (long long)gridDim.x * blockDim.x) {
+        const uint32_t t = g.flags[c] & kTypeMask;
+        float u[3] = {0.0f, 0.0f, 0.0f};
+        if (DIM == 2) {
+            if (t == kInletLeft) u[0] = bc.v[0];
+            else if (t == kInletDown) u[1] = bc.v[1];
+            else if (t == kInletRight) u[0] = -bc.v[2];
+            else if (t == kInletUp) u[1] = -bc.v[3];
+        } else {
+            if (t == kInletLeft) u[0] = bc.v[0];
+            else if (t == kInletDown) u[2] = bc.v[1];
+            else if (t == kInletRight) u[0] = -bc.v[2];
+            else if (t == kInletUp) u[2] = -bc.v[3];
+            else if (t == kInletFront) u[1] = bc.v[4];
+            else if (t == kInletBack) u[1] = -bc.v[5];
+        }
+        float m[NM];
+        m[0] = 1.0f;
+        for (int a = 0; a < DIM; ++a) m[1 + a] = u[a];
+        for (int k = DIM + 1; k < NM; ++k) m[k] = u[MomentLayout<DIM>::pa(k)] * u[MomentLayout<DIM>::pb(k)];
+        T *pa[NM], *pb[NM];
+        for (int k = 0; k < NM; ++k) { pa[k] = g.dst + (size_t)k * g.ncell; pb[k] = other + (size_t)k * g.ncell; }
+        encode_store<DIM, T>(m, pa, (uint32_t)c, g.codec);
+        encode_store<DIM, T>(m, pb, (uint32_t)c, g.codec);
+    }
+}
+
+template <int DIM, typename T>
+cudaError_t launch_initialize(const GridArgs<T> &g, T *other, const float *bcvel, cudaStream_t st)
+{
+    Vel6 bc;
+    for (int i = 0; i < 6; ++i) bc.v[i] = bcvel[i];
+    int grid = (int)std::min<long long>(((long long)g.ncell + 255) / 256, 148LL * 16);
+    initialize_kernel<DIM, T><<<grid, 256, 0, st>>>(g, other, bc);
+    return cudaGetLastError();
+}
+
+// updateSolidFlagKernel / resetSolidFlagKernel with the even-odd crossing
+// test of SolidGeometryProxy_Device<2>::isInside (:126-144), each operation
+// explicitly rounded so the mask matches the CPU oracle exactly.
+__global__ void fill_solid2_kernel(uint8_t *flags, int nx, int ny, float cl, SurfaceArgs s)
+{
+    using namespace geom;
+    const long long n = (long long)nx * ny;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        uint32_t t = flags[c] & kTypeMask;
+        if (t != kFluid && t != kSolidDynamic) continue;
+        const int x = (int)(c % nx), y = (int)(c / nx);
+        const float px = mul(add((float)x, 0.5f), cl), py = mul(add((float)y, 0.5f), cl);
+        bool in = false;
+        for (int i = 0; i < s.ne; ++i) {
+            uint32_t a = s.E[2 * i], b = s.E[2 * i + 1];
+            float sx = s.V[2 * a], sy = s.V[2 * a + 1], tx = s.V[2 * b], ty = s.V[2 * b + 1];
+            if ((sy < py && ty >= py) || (sy >= py && ty < py))
+                in ^= (add(sx, dvd(mul(sub(py, sy), sub(tx, sx)), sub(ty, sy))) > px);
+        }
+        flags[c] = in ? kSolidDynamic : kFluid;
+    }
+}
+
+cudaError_t launch_fill_solid2(uint8_t *flags, int nx, int ny, float cl, const SurfaceArgs &s, cudaStream_t st)
+{
+    long long n = (long long)nx * ny;
+    int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    fill_solid2_kernel<<<grid, 256, 0, st>>>(flags, nx, ny, cl, s);
+    return cudaGetLastError();
+}
+
+// FP32 AoS/SoA <-> device storage (SoA planes, possibly encoded)
+template <int DIM, typename T>
+__global__ void convert_in_kernel(const float *in, bool aos, T *out, uint32_t ncell, Codec cdc)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        float m[NM];
+        for (int k = 0; k < NM; ++k) m[k] = aos ? in[c * NM + k] : in[(size_t)k * ncell + c];
+        T *pl[NM];
+        for (int k = 0; k < NM; ++k) pl[k] = out + (size_t)k * ncell;
+        encode_store<DIM, T>(m, pl, (uint32_t)c, cdc);
+    }
+}
+
+template <int DIM, typename T>
+__global__ void convert_out_kernel(const T *in, float *out, bool aos, uint32_t ncell, Codec cdc)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        float m[NM];
+        load_moments<DIM, T>(m, in, ncell, (uint32_t)c, cdc);
+        for (int k = 0; k < NM; ++k) {
+            if (aos) out[c * NM + k] = m[k];
+            else out[(size_t)k * ncell + c] = m[k];
+        }
+    }
+}
+
+template <int DIM, typename T>
+cudaError_t launch_convert_in(const float *in, bool aos, T *out, uint32_t ncell, Codec c, cudaStream_t st)
+{
+    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, 148LL * 16);
+    convert_in_kernel<DIM, T><<<grid, 256, 0, st>>>(in, aos, out, ncell, c);
+    return cudaGetLastError();
+}
+template <int DIM, typename T>
+cudaError_t launch_convert_out(const T *in, float *out, bool aos, uint32_t ncell, Codec c, cudaStream_t st)
+{
+    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, 148LL * 16);
+    convert_out_kernel<DIM, T><<<grid, 256, 0, st>>>(in, out, aos, ncell, c);
+    return cudaGetLastError();
+}
+
+#define FFS_INST_AUX(DIM, T)                                                                                           \
+    template cudaError_t launch_initialize<DIM, T>(const GridArgs<T> &, T *, const float *, cudaStream_t);            \
+    template cudaError_t launch_convert_in<DIM, T>(const float *, bool, T *, uint32_t, Codec, cudaStream_t);          \
+    template cudaError_t launch_convert_out<DIM, T>(const T *, float *, bool, uint32_t, Codec, cudaStream_t);
+FFS_INST_AUX(2, float)
+FFS_INST_AUX(2, __half)
+FFS_INST_AUX(2, __nv_bfloat16)
+FFS_INST_AUX(3, float)
+FFS_INST_AUX(3, __half)
+FFS_INST_AUX(3, __nv_bfloat16)
+
+} // namespace fflbm

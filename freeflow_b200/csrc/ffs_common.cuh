@@ -1,0 +1,218 @@
+// Common device definitions for the B200 moment-encoded LBM fluid step.
+//
+// Lattices (same direction numbering as the reference, so link indices,
+// inverse directions and the AoS layout exchanged through the C ABI agree):
+//   D2Q9  include/FSI_Simulator/lbm/LbmConstants.hpp:48-54
+//   D3Q27 include/FSI_Simulator/lbm/LbmConstants.hpp:24-35
+// Node flags: include/FSI_Simulator/lbm/LbmDataTypes.cuh:17-56.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+
+namespace fflbm {
+
+// ---------------------------------------------------------------- lattices
+template <int DIM> struct Lattice;
+
+template <> struct Lattice<2> {
+    static constexpr int Q = 9, NM = 6;
+    static __host__ __device__ constexpr int cx(int i) { return i == 1 || i == 5 || i == 8 ? 1 : (i == 3 || i == 6 || i == 7 ? -1 : 0); }
+    static __host__ __device__ constexpr int cy(int i) { return i == 2 || i == 5 || i == 6 ? 1 : (i == 4 || i == 7 || i == 8 ? -1 : 0); }
+    static __host__ __device__ constexpr int cz(int) { return 0; }
+    static __host__ __device__ constexpr int inv(int i) { return i == 0 ? 0 : (i <= 4 ? ((i + 1) % 4) + 1 : ((i - 3) % 4) + 5); }
+};
+
+template <> struct Lattice<3> {
+    static constexpr int Q = 27, NM = 10;
+    static __host__ __device__ constexpr int cx(int i)
+    {
+        constexpr int t[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+        return t[i];
+    }
+    static __host__ __device__ constexpr int cy(int i)
+    {
+        constexpr int t[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+        return t[i];
+    }
+    static __host__ __device__ constexpr int cz(int i)
+    {
+        constexpr int t[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+        return t[i];
+    }
+    // reference numbering pairs i with i+1 (odd i) after the rest population
+    static __host__ __device__ constexpr int inv(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+};
+
+// direction index of the velocity (cx, cy, cz); -1 if none
+template <int DIM> __host__ __device__ constexpr int dir_of(int x, int y, int z)
+{
+    for (int i = 0; i < Lattice<DIM>::Q; ++i)
+        if (Lattice<DIM>::cx(i) == x && Lattice<DIM>::cy(i) == y && Lattice<DIM>::cz(i) == z) return i;
+    return -1;
+}
+
+// Direction index by velocity, [kz][ky][kx] with k = c + 1, filled at compile
+// time so that unrolled loops over (kx, ky, kz) index it with constants.
+template <int DIM> struct DirTable {
+    int v[3][3][3];
+    __host__ __device__ constexpr DirTable() : v{}
+    {
+        for (int kz = 0; kz < 3; ++kz)
+            for (int ky = 0; ky < 3; ++ky)
+                for (int kx = 0; kx < 3; ++kx) v[kz][ky][kx] = dir_of<DIM>(kx - 1, ky - 1, kz - 1);
+    }
+};
+template <int DIM> __host__ __device__ constexpr int dir_index(int kx, int ky, int kz)
+{
+    constexpr DirTable<DIM> t{};
+    return t.v[kz][ky][kx];
+}
+
+// ------------------------------------------------------------------- flags
+enum Flag : uint8_t {
+    kInvalid = 0, kFluid = 1, kFluidRest = 2, kSolid = 3, kSolidDynamic = 4, kWall = 5,
+    kWallLeft = 6, kWallRight = 7, kWallFront = 8, kWallBack = 9, kWallDown = 10, kWallUp = 11,
+    kWallCorner = 12, kInletLeft = 13, kInletRight = 14, kInletUp = 15, kInletDown = 16,
+    kInletFront = 17, kInletBack = 18, kOutletLeft = 19, kOutletRight = 20, kOutletUp = 21,
+    kOutletDown = 22, kOutletFront = 23, kOutletBack = 24, kReceptor = 25, kDeactivated = 26, kSmoke = 27,
+};
+
+// The device flag byte keeps the node type in its low 5 bits and three
+// derived bits the kernels use to stay on the fast path:
+constexpr uint8_t kTypeMask = 0x1F;
+constexpr uint8_t kBitOutletSrc = 0x20; // fluid cell that feeds a neighbouring outlet node
+constexpr uint8_t kBitNearWall = 0x40;  // some neighbour x - c_i is a bounce-back node
+constexpr uint8_t kBitLink = 0x80;      // cell has moving-boundary links this step
+
+// bounce-back node types: FsiCoupling2D.cu:171-176, FsiCoupling3D.cu:209-216
+template <int DIM> __host__ __device__ inline bool is_bounce_back(uint32_t t)
+{
+    uint32_t m = (1u << kSolid) | (1u << kWall) | (1u << kWallLeft) | (1u << kWallRight) | (1u << kWallUp) | (1u << kWallDown);
+    if (DIM == 3) m |= (1u << kWallFront) | (1u << kWallBack);
+    return t < 32 && ((m >> t) & 1u);
+}
+
+__host__ __device__ inline bool is_updated(uint32_t t) { return t == kFluid || t == kSolidDynamic; }
+
+// ------------------------------------------------------------ status bits
+enum StatusBits : uint32_t {
+    kStatusNonFinite = 1u << 0,     // a fluid update produced a non-finite density
+    kStatusLinkOverflow = 1u << 1,  // link hash table full; some links were dropped
+    kStatusForceRange = 1u << 2,    // a force contribution exceeded the fixed-point range
+    kStatusBadElement = 1u << 3,    // element index out of range in the surface
+};
+
+// ---------------------------------------------------------------- storage
+enum Storage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
+
+// Reduced-precision storage keeps scaled deviations from equilibrium:
+//   rho - 1,  u * su,  (pi_ab - u_a u_b) * sp
+// su and sp are powers of two, so scaling is exact; decode(encode(x)) loses
+// only the 11-bit (fp16) or 8-bit (bf16) rounding of the deviation.
+struct Codec {
+    float su, inv_su, sp, inv_sp;
+};
+
+template <typename T> struct StorageTraits;
+template <> struct StorageTraits<float> {
+    static constexpr bool kEncoded = false;
+    __device__ static float to(float v) { return v; }
+    __device__ static float from(float v) { return v; }
+};
+template <> struct StorageTraits<__half> {
+    static constexpr bool kEncoded = true;
+    __device__ static __half to(float v) { return __float2half_rn(v); }
+    __device__ static float from(__half v) { return __half2float(v); }
+};
+template <> struct StorageTraits<__nv_bfloat16> {
+    static constexpr bool kEncoded = true;
+    __device__ static __nv_bfloat16 to(float v) { return __float2bfloat16_rn(v); }
+    __device__ static float from(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
+
+// Index of pi_ab in the moment vector and the (a, b) pair of each stored
+// second moment, for the encoding above.
+template <int DIM> struct MomentLayout;
+template <> struct MomentLayout<2> {
+    // [rho, ux, uy, pixx, piyy, pixy]
+    static __host__ __device__ constexpr int pa(int k) { return k == 3 ? 0 : (k == 4 ? 1 : 0); }
+    static __host__ __device__ constexpr int pb(int k) { return k == 3 ? 0 : (k == 4 ? 1 : 1); }
+};
+template <> struct MomentLayout<3> {
+    // [rho, ux, uy, uz, pixx, piyy, pizz, pixy, piyz, pixz]
+    static __host__ __device__ constexpr int pa(int k) { return k == 4 ? 0 : k == 5 ? 1 : k == 6 ? 2 : k == 7 ? 0 : k == 8 ? 1 : 0; }
+    static __host__ __device__ constexpr int pb(int k) { return k == 4 ? 0 : k == 5 ? 1 : k == 6 ? 2 : k == 7 ? 1 : k == 8 ? 2 : 2; }
+};
+
+// Decode a stored moment vector (already loaded as floats) in place.
+template <int DIM, typename T>
+__device__ __forceinline__ void decode_moments(float *m, const Codec &c)
+{
+    if constexpr (StorageTraits<T>::kEncoded) {
+        constexpr int NM = Lattice<DIM>::NM;
+        m[0] = 1.0f + m[0];
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) m[1 + a] *= c.inv_su;
+#pragma unroll
+        for (int k = DIM + 1; k < NM; ++k)
+            m[k] = fmaf(m[k], c.inv_sp, m[1 + MomentLayout<DIM>::pa(k)] * m[1 + MomentLayout<DIM>::pb(k)]);
+    }
+}
+
+// Encode m (floats) to storage; the u used for the stress deviation is the
+// rounded one, so that decode() reproduces pi up to the deviation's rounding.
+template <int DIM, typename T>
+__device__ __forceinline__ void encode_store(const float *m, T *const *planes, uint32_t idx, const Codec &c)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    if constexpr (!StorageTraits<T>::kEncoded) {
+#pragma unroll
+        for (int k = 0; k < NM; ++k) planes[k][idx] = StorageTraits<T>::to(m[k]);
+    } else {
+        float ud[DIM];
+        planes[0][idx] = StorageTraits<T>::to(m[0] - 1.0f);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            T s = StorageTraits<T>::to(m[1 + a] * c.su);
+            planes[1 + a][idx] = s;
+            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
+        }
+#pragma unroll
+        for (int k = DIM + 1; k < NM; ++k)
+            planes[k][idx] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+    }
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ void load_moments(float *m, const T *base, uint32_t ncell, uint32_t idx, const Codec &c)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) m[k] = StorageTraits<T>::from(base[(size_t)k * ncell + idx]);
+    decode_moments<DIM, T>(m, c);
+}
+
+struct Vel6 {
+    float v[6];
+};
+
+// --------------------------------------------------------- grid descriptor
+// Everything one fluid grid's kernels need, passed by value.
+template <typename T> struct GridArgs {
+    int nx, ny, nz;
+    uint32_t ncell;
+    int periodic;            // bit0 x, bit1 y, bit2 z wrap the pull halo (reference: clamp)
+    int half_pops;           // D2Q9: round reconstructed populations to binary16 (reference tile)
+    float omega;
+    Codec codec;
+    const T *src;            // SoA: moment k of cell c at src[k * ncell + c]
+    T *dst;
+    const uint8_t *flags;
+    const uint32_t *wallmask; // per-cell bounce-back direction mask (read only for near-wall cells)
+    uint32_t *status;
+};
+
+} // namespace fflbm

@@ -1,0 +1,271 @@
+// Moment-space math of the fluid step: third-order Hermite reconstruction of
+// populations from moments, raw moments of populations, and the moment-space
+// collision with re-encoding.
+//
+// Reference semantics (FreeFlow):
+//   reconstruction  src/lbm/LbmUtilsFunc.cu:212-335 (D3Q27), :476-510 (D2Q9)
+//   collision       src/lbm/LbmUtilsFunc.cu:337-414 (D3Q27), :512-543 (D2Q9)
+//   re-encode       src/core/FsiCoupling2D.cu:243-252, src/core/FsiCoupling3D.cu:310-320
+//
+// The reference writes every population as its own explicit sum.  Here the
+// expansion is evaluated as what it is, a tensor product of the 1D basis
+// {1, c, g(c)} with g(+-1) = 1, g(0) = -1/2 and weights w(0) = 2/3,
+// w(+-1) = 1/6: the coefficient A_pqr multiplies phi_p(cx) phi_q(cy) phi_r(cz),
+// so the 27 (9) populations come out of three (two) small 1D passes, and the
+// raw moments go back through the matching forward passes.  The results equal
+// the reference's up to FP32 rounding order.
+#pragma once
+#include "ffs_common.cuh"
+
+namespace fflbm {
+
+// v[0..2] = a0 + a1*c + a2*g(c) at c = -1, 0, +1
+__device__ __forceinline__ void herm3(float a0, float a1, float a2, float *v)
+{
+    float t = a0 + a2;
+    v[0] = t - a1;
+    v[1] = fmaf(-0.5f, a2, a0);
+    v[2] = t + a1;
+}
+// v[0..2] = a0 + a1*c at c = -1, 0, +1
+__device__ __forceinline__ void herm2(float a0, float a1, float *v)
+{
+    v[0] = a0 - a1;
+    v[1] = a0;
+    v[2] = a0 + a1;
+}
+
+__host__ __device__ constexpr float wgt1(int k) { return k == 1 ? 2.0f / 3.0f : 1.0f / 6.0f; }
+
+// Hermite coefficients of one cell (the reference's m1, m2 and Q terms).
+template <int DIM> struct Coef;
+
+template <> struct Coef<2> {
+    float rho, m1x, m1y, m2xx, m2yy, m2xy, qxxy, qxyy;
+    // m = [rho, ux, uy, pixx, piyy, pixy]; the D2Q9 reference omits rho on
+    // the pi terms of Q (LbmUtilsFunc.cu:488-490).
+    __device__ __forceinline__ void make(const float *m)
+    {
+        float r = m[0], ux = m[1], uy = m[2], pxx = m[3], pyy = m[4], pxy = m[5];
+        float r3 = 3.0f * r;
+        rho = r;
+        m1x = r3 * ux; m1y = r3 * uy;
+        m2xx = r3 * pxx; m2yy = r3 * pyy; m2xy = 9.0f * r * pxy;
+        float rux = r * ux, ruy = r * uy;
+        qxxy = 9.0f * fmaf(pxx, uy, 2.0f * ux * (pxy - rux * uy));
+        qxyy = 9.0f * fmaf(pyy, ux, 2.0f * uy * (pxy - ruy * ux));
+    }
+    // all nine populations, reference numbering
+    __device__ __forceinline__ void populations(float *f) const
+    {
+        float C0[3], C1[3], C2[3];
+        herm3(rho, m1y, m2yy, C0);
+        herm3(m1x, m2xy, qxyy, C1);
+        herm2(m2xx, qxxy, C2);
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            float F[3];
+            herm3(C0[ky], C1[ky], C2[ky], F);
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const int i = dir_index<2>(kx, ky, 1);
+                f[i] = (wgt1(kx) * wgt1(ky)) * F[kx];
+            }
+        }
+    }
+    // one population, direction given at run time
+    __device__ __forceinline__ float population(int cx, int cy, int) const
+    {
+        float gx = cx ? 1.0f : -0.5f, gy = cy ? 1.0f : -0.5f;
+        float fx = (float)cx, fy = (float)cy;
+        float s = rho;
+        s = fmaf(m1x, fx, s); s = fmaf(m1y, fy, s);
+        s = fmaf(m2xx, gx, s); s = fmaf(m2yy, gy, s);
+        s = fmaf(m2xy, fx * fy, s);
+        s = fmaf(qxxy, gx * fy, s); s = fmaf(qxyy, fx * gy, s);
+        float w = (cx ? 1.0f / 6.0f : 2.0f / 3.0f) * (cy ? 1.0f / 6.0f : 2.0f / 3.0f);
+        return w * s;
+    }
+};
+
+template <> struct Coef<3> {
+    float rho, m1x, m1y, m1z, m2xx, m2yy, m2zz, m2xy, m2yz, m2xz;
+    float qxxy, qxyy, qxxz, qxzz, qyyz, qyzz, qxyz;
+    // m = [rho, ux, uy, uz, pixx, piyy, pizz, pixy, piyz, pixz]
+    __device__ __forceinline__ void make(const float *m)
+    {
+        float r = m[0], ux = m[1], uy = m[2], uz = m[3];
+        float pxx = m[4], pyy = m[5], pzz = m[6], pxy = m[7], pyz = m[8], pxz = m[9];
+        float r3 = 3.0f * r, r9 = 9.0f * r;
+        rho = r;
+        m1x = r3 * ux; m1y = r3 * uy; m1z = r3 * uz;
+        m2xx = r3 * pxx; m2yy = r3 * pyy; m2zz = r3 * pzz;
+        m2xy = r9 * pxy; m2yz = r9 * pyz; m2xz = r9 * pxz;
+        // Q_aab = 9 rho (pi_aa u_b + 2 u_a (pi_ab - u_a u_b))
+        float dxy = fmaf(-ux, uy, pxy), dyz = fmaf(-uy, uz, pyz), dxz = fmaf(-ux, uz, pxz);
+        float r18 = 2.0f * r9;
+        qxxy = fmaf(r9 * pxx, uy, r18 * ux * dxy);
+        qxyy = fmaf(r9 * pyy, ux, r18 * uy * dxy);
+        qxxz = fmaf(r9 * pxx, uz, r18 * ux * dxz);
+        qxzz = fmaf(r9 * pzz, ux, r18 * uz * dxz);
+        qyyz = fmaf(r9 * pyy, uz, r18 * uy * dyz);
+        qyzz = fmaf(r9 * pzz, uy, r18 * uz * dyz);
+        // Q_xyz = 27 rho (pi_xy uz + pi_yz ux + pi_xz uy - 2 ux uy uz)
+        float t = fmaf(pxy, uz, fmaf(pyz, ux, pxz * uy));
+        qxyz = 27.0f * r * fmaf(-2.0f * ux * uy, uz, t);
+    }
+    // The 27 populations, sorted by slice: out[kz][ky][kx] with k = c + 1.
+    __device__ __forceinline__ void populations_xyz(float (*out)[3][3]) const
+    {
+        float B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
+        herm3(rho, m1z, m2zz, B00);
+        herm3(m1x, m2xz, qxzz, B10);
+        herm3(m1y, m2yz, qyzz, B01);
+        herm2(m2xx, qxxz, B20);
+        herm2(m2yy, qyyz, B02);
+        herm2(m2xy, qxyz, B11);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            float C0[3], C1[3], C2[3];
+            herm3(B00[kz], B01[kz], B02[kz], C0);
+            herm3(B10[kz], B11[kz], qxyy, C1);
+            herm2(B20[kz], qxxy, C2);
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                float F[3];
+                herm3(C0[ky], C1[ky], C2[ky], F);
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = (wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx];
+            }
+        }
+    }
+    __device__ __forceinline__ void populations(float *f) const
+    {
+        float o[3][3][3];
+        populations_xyz(o);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) f[dir_index<3>(kx, ky, kz)] = o[kz][ky][kx];
+    }
+    __device__ __forceinline__ float population(int cx, int cy, int cz) const
+    {
+        float gx = cx ? 1.0f : -0.5f, gy = cy ? 1.0f : -0.5f, gz = cz ? 1.0f : -0.5f;
+        float fx = (float)cx, fy = (float)cy, fz = (float)cz;
+        float s = rho;
+        s = fmaf(m1x, fx, s); s = fmaf(m1y, fy, s); s = fmaf(m1z, fz, s);
+        s = fmaf(m2xx, gx, s); s = fmaf(m2yy, gy, s); s = fmaf(m2zz, gz, s);
+        s = fmaf(m2xy, fx * fy, s); s = fmaf(m2yz, fy * fz, s); s = fmaf(m2xz, fx * fz, s);
+        s = fmaf(qxxy, gx * fy, s); s = fmaf(qxyy, fx * gy, s);
+        s = fmaf(qxxz, gx * fz, s); s = fmaf(qxzz, fx * gz, s);
+        s = fmaf(qyyz, gy * fz, s); s = fmaf(qyzz, fy * gz, s);
+        s = fmaf(qxyz, fx * fy * fz, s);
+        float w = (cx ? 1.0f / 6.0f : 2.0f / 3.0f) * (cy ? 1.0f / 6.0f : 2.0f / 3.0f) * (cz ? 1.0f / 6.0f : 2.0f / 3.0f);
+        return w * s;
+    }
+};
+
+// ------------------------------------------------------------ raw moments
+// R = {rho, jx, jy[, jz], Pxx, Pyy[, Pzz], Pxy[, Pyz, Pxz]} (raw sums)
+__device__ __forceinline__ void raw_moments2(const float *f, float *R)
+{
+    // rows by cy: (f(-1), f(0), f(+1))
+    float s0 = f[1] + f[3], d0 = f[1] - f[3], x00 = f[0] + s0;   // cy = 0
+    float s1 = f[5] + f[6], d1 = f[5] - f[6], x01 = f[2] + s1;   // cy = +1
+    float sm = f[8] + f[7], dm = f[8] - f[7], x0m = f[4] + sm;   // cy = -1
+    float sy = x01 + x0m;
+    R[0] = x00 + sy;            // rho
+    R[1] = d0 + (d1 + dm);      // jx
+    R[2] = x01 - x0m;           // jy
+    R[3] = s0 + (s1 + sm);      // Pxx
+    R[4] = sy;                  // Pyy
+    R[5] = d1 - dm;             // Pxy
+}
+
+__device__ __forceinline__ void raw_moments3(const float (*F)[3][3], float *R)
+{
+    // F[kz][ky][kx]; stage x
+    float X0[3][3], X1[3][3], X2[3][3];
+#pragma unroll
+    for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            float s = F[kz][ky][2] + F[kz][ky][0];
+            X1[kz][ky] = F[kz][ky][2] - F[kz][ky][0];
+            X2[kz][ky] = s;
+            X0[kz][ky] = F[kz][ky][1] + s;
+        }
+    // stage y: Y[p][q][kz]
+    float Y00[3], Y01[3], Y02[3], Y10[3], Y11[3], Y20[3];
+#pragma unroll
+    for (int kz = 0; kz < 3; ++kz) {
+        float s0 = X0[kz][2] + X0[kz][0];
+        Y00[kz] = X0[kz][1] + s0; Y01[kz] = X0[kz][2] - X0[kz][0]; Y02[kz] = s0;
+        float s1 = X1[kz][2] + X1[kz][0];
+        Y10[kz] = X1[kz][1] + s1; Y11[kz] = X1[kz][2] - X1[kz][0];
+        Y20[kz] = X2[kz][1] + (X2[kz][2] + X2[kz][0]);
+    }
+    float s = Y00[2] + Y00[0];
+    R[0] = Y00[1] + s;                    // rho   M000
+    R[3] = Y00[2] - Y00[0];               // jz    M001
+    R[6] = s;                             // Pzz   M002
+    R[2] = Y01[1] + (Y01[2] + Y01[0]);    // jy    M010
+    R[8] = Y01[2] - Y01[0];               // Pyz   M011
+    R[5] = Y02[1] + (Y02[2] + Y02[0]);    // Pyy   M020
+    R[1] = Y10[1] + (Y10[2] + Y10[0]);    // jx    M100
+    R[9] = Y10[2] - Y10[0];               // Pxz   M101
+    R[7] = Y11[1] + (Y11[2] + Y11[0]);    // Pxy   M110
+    R[4] = Y20[1] + (Y20[2] + Y20[0]);    // Pxx   M200
+}
+
+// ------------------------------------------------------------- collision
+// Input: raw moments R (see above).  Output: the stored moment vector
+// [rho, u, pi] with pi = Pi'/rho - c_s^2 delta, where Pi' is the relaxed
+// second moment of LbmUtilsFunc.cu:337-414 / :512-543 (body force is zero on
+// this path: FsiCoupling2D.cu:227-228; the 3D body-force field is never set,
+// LbmFlowField3D.cpp:85-86).  Written in the algebraically equal form
+// pi' = (dev * (1 - omega) / rho) + equilibrium part, which avoids
+// subtracting c_s^2 from a value near c_s^2.
+__device__ __forceinline__ void collide2(const float *R, float omega, float *m)
+{
+    float rho = R[0];
+    float ir = 1.0f / rho;
+    float ux = R[1] * ir, uy = R[2] * ir;
+    float omw = 1.0f - omega;
+    float ux2 = ux * ux, uy2 = uy * uy;
+    float half_u2 = 0.5f * (ux2 + uy2);
+    float dev = 0.5f * (R[3] - R[4]) * omw * ir;
+    float an = 0.5f * omega * (ux2 - uy2);
+    m[0] = rho; m[1] = ux; m[2] = uy;
+    m[3] = half_u2 + dev + an;
+    m[4] = half_u2 - dev - an;
+    m[5] = fmaf(omw * R[5], ir, omega * ux * uy);
+}
+
+__device__ __forceinline__ void collide3(const float *R, float omega, float *m)
+{
+    const float third = 1.0f / 3.0f;
+    float rho = R[0];
+    float ir = 1.0f / rho;
+    float ux = R[1] * ir, uy = R[2] * ir, uz = R[3] * ir;
+    float omw = 1.0f - omega;
+    float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    float u2_3 = (ux2 + uy2 + uz2) * third;
+    float tr_3 = (R[4] + R[5] + R[6]) * third;
+    float k = omw * ir;
+    m[0] = rho; m[1] = ux; m[2] = uy; m[3] = uz;
+    // pi'_aa = u^2/3 + (1-w)(P_aa - tr/3)/rho + w (u_a^2 - u^2/3)
+    m[4] = fmaf(k, R[4] - tr_3, fmaf(omega, ux2 - u2_3, u2_3));
+    m[5] = fmaf(k, R[5] - tr_3, fmaf(omega, uy2 - u2_3, u2_3));
+    m[6] = fmaf(k, R[6] - tr_3, fmaf(omega, uz2 - u2_3, u2_3));
+    // pi'_ab = (1-w) P_ab / rho + w u_a u_b
+    m[7] = fmaf(k, R[7], omega * ux * uy);
+    m[8] = fmaf(k, R[8], omega * uy * uz);
+    m[9] = fmaf(k, R[9], omega * ux * uz);
+}
+
+__device__ __forceinline__ float round_half(float v) { return __half2float(__float2half_rn(v)); }
+
+} // namespace fflbm

@@ -1,0 +1,216 @@
+"""Python handle on one fluid grid, calling the C ABI (``include/ffs_lbm.h``).
+
+This is the Python-side equivalent of FreeFlow's ``LbmFlowField2D/3D`` plus
+``fsi_coupling::solveLbmAndFsiStep2D/3D``.  Device memory for surfaces comes
+from torch tensors (plumbing only); every computation runs in the CUDA
+kernels of ``libffs_lbm.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi as A
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(0)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    h = getattr(stream, "cuda_stream", None)
+    if h is not None:
+        return C.c_void_p(int(h))
+    return C.c_void_p(int(stream))
+
+
+def _np_ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class DeviceSurface:
+    """Surface arrays on the device, the SolidGeometryProxy_Device view.
+
+    vertices / velocities: (nv, dim) float32, physical units; elements:
+    (ne, dim) uint32 vertex indices (segments in 2D, triangles in 3D).
+    ``forces`` (nv, dim) float32 accumulates the fluid force (+=) and
+    ``forces64`` (optional) the same in float64.
+    """
+
+    def __init__(self, vertices, velocities, elements, device="cuda", with_forces64=False):
+        import torch
+
+        v = torch.as_tensor(np.ascontiguousarray(vertices, dtype=np.float32), device=device)
+        self.dim = int(v.shape[1])
+        self.vertices = v.contiguous()
+        self.velocities = torch.as_tensor(np.ascontiguousarray(velocities, dtype=np.float32), device=device).contiguous()
+        e = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1, self.dim)
+        # torch has no uint32 arithmetic we need; keep raw bytes in int32
+        self.elements = torch.as_tensor(e.view(np.int32), device=device).contiguous()
+        self.forces = torch.zeros_like(self.vertices)
+        self.forces64 = torch.zeros(self.vertices.shape, dtype=torch.float64, device=device) if with_forces64 else None
+        assert self.velocities.shape == self.vertices.shape
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.vertices.shape[0])
+
+    @property
+    def num_elements(self) -> int:
+        return int(self.elements.shape[0])
+
+    def update(self, vertices=None, velocities=None):
+        if vertices is not None:
+            self.vertices.copy_(self._t(vertices))
+        if velocities is not None:
+            self.velocities.copy_(self._t(velocities))
+
+    def _t(self, a):
+        import torch
+        if isinstance(a, torch.Tensor):
+            return a.to(self.vertices.device, torch.float32)
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32))
+
+    def c_struct(self) -> A.Surface:
+        s = A.Surface()
+        s.dim = self.dim
+        s.vertices = self.vertices.data_ptr()
+        s.velocities = self.velocities.data_ptr()
+        s.elements = self.elements.data_ptr()
+        s.num_vertices = self.num_vertices
+        s.num_elements = self.num_elements
+        s.forces = self.forces.data_ptr()
+        s.forces64 = self.forces64.data_ptr() if self.forces64 is not None else None
+        return s
+
+
+@dataclass
+class GridInfo:
+    ncell: int
+    nm: int
+    q: int
+    omega: float
+    cf: float
+
+
+class FluidGrid:
+    """One D2Q9 / D3Q27 fluid grid resident on the GPU."""
+
+    def __init__(self, dim: int, nx: int, ny: int, nz: int = 1, fluid_viscosity: float = 0.001,
+                 fluid_density: float = 1000.0, fluid_dx: float = 1.0, dt: float = 0.001,
+                 boundary_velocities=None, storage: str = "f32", periodic: int = 0,
+                 ref_half_populations: bool = False):
+        L = A.load()
+        d = A.LbmDesc()
+        d.dim, d.nx, d.ny, d.nz = dim, nx, ny, (1 if dim == 2 else nz)
+        d.fluid_viscosity, d.fluid_density, d.fluid_dx, d.dt = fluid_viscosity, fluid_density, fluid_dx, dt
+        bc = list(boundary_velocities or [])
+        for i in range(6):
+            d.boundary_velocities[i] = float(bc[i]) if i < len(bc) else 0.0
+        d.storage = A.STORAGE[storage] if isinstance(storage, str) else int(storage)
+        d.periodic_mask = int(periodic)
+        d.ref_half_populations = int(bool(ref_half_populations))
+        self._h = C.c_void_p()
+        A.check(L.ffs_lbm_create(C.byref(d), C.byref(self._h)), "ffs_lbm_create")
+        self.dim, self.nx, self.ny, self.nz = dim, nx, ny, d.nz
+        self.storage = storage
+        self.info = self._info()
+
+    # -- life cycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            A.load().ffs_lbm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _info(self) -> GridInfo:
+        n = C.c_int64()
+        nm, q = C.c_int(), C.c_int()
+        om, cf = C.c_double(), C.c_double()
+        A.check(A.load().ffs_lbm_get_info(self._h, C.byref(n), C.byref(nm), C.byref(q), C.byref(om), C.byref(cf)),
+                "ffs_lbm_get_info")
+        return GridInfo(n.value, nm.value, q.value, om.value, cf.value)
+
+    @property
+    def ncell(self) -> int:
+        return self.info.ncell
+
+    @property
+    def nm(self) -> int:
+        return self.info.nm
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- state ---------------------------------------------------------------
+    def set_flags(self, flags, stream=None):
+        f = np.ascontiguousarray(flags, dtype=np.uint8).reshape(-1)
+        assert f.size == self.ncell
+        A.check(A.load().ffs_lbm_set_flags(self._h, _np_ptr(f), A.MEM_HOST, _stream_handle(stream)), "set_flags")
+
+    def get_flags(self, stream=None) -> np.ndarray:
+        f = np.zeros(self.ncell, dtype=np.uint8)
+        A.check(A.load().ffs_lbm_get_flags(self._h, _np_ptr(f), A.MEM_HOST, _stream_handle(stream)), "get_flags")
+        return f
+
+    def initialize(self, stream=None):
+        A.check(A.load().ffs_lbm_initialize(self._h, _stream_handle(stream)), "initialize")
+
+    def set_moments(self, m, which: int = A.BUF_BOTH, layout: int = A.LAYOUT_AOS, stream=None):
+        a = np.ascontiguousarray(m, dtype=np.float32).reshape(-1)
+        assert a.size == self.ncell * self.nm
+        A.check(A.load().ffs_lbm_set_moments(self._h, _np_ptr(a), layout, A.MEM_HOST, which, _stream_handle(stream)),
+                "set_moments")
+
+    def get_moments(self, which: int = A.BUF_CURRENT, layout: int = A.LAYOUT_AOS, stream=None) -> np.ndarray:
+        a = np.zeros(self.ncell * self.nm, dtype=np.float32)
+        A.check(A.load().ffs_lbm_get_moments(self._h, _np_ptr(a), layout, A.MEM_HOST, which, _stream_handle(stream)),
+                "get_moments")
+        return a.reshape(self.ncell, self.nm) if layout == A.LAYOUT_AOS else a.reshape(self.nm, self.ncell)
+
+    def reserve_surface(self, max_vertices: int, max_link_cells: int):
+        A.check(A.load().ffs_lbm_reserve_surface(self._h, int(max_vertices), int(max_link_cells)), "reserve_surface")
+
+    # -- stepping -------------------------------------------------------------
+    def step(self, surface: DeviceSurface | None = None, stream=None):
+        s = surface.c_struct() if surface is not None else None
+        A.check(A.load().ffs_lbm_step(self._h, C.byref(s) if s is not None else None, _stream_handle(stream)), "step")
+
+    def fill_solid(self, surface: DeviceSurface, stream=None):
+        s = surface.c_struct()
+        A.check(A.load().ffs_lbm_fill_solid(self._h, C.byref(s), _stream_handle(stream)), "fill_solid")
+
+    def status(self, clear: bool = True, stream=None) -> int:
+        v = C.c_uint32()
+        A.check(A.load().ffs_lbm_get_status(self._h, C.byref(v), int(clear), _stream_handle(stream)), "get_status")
+        return int(v.value)
+
+    def profile(self, enable: bool = True):
+        """Start/stop per-stage CUDA-event timing of the steps."""
+        A.check(A.load().ffs_lbm_profile_enable(self._h, int(bool(enable))), "profile_enable")
+
+    def profile_read(self, reset: bool = True) -> dict:
+        """{stage: (milliseconds, launches)} summed since the last reset."""
+        p = A.Profile()
+        A.check(A.load().ffs_lbm_profile_read(self._h, C.byref(p), int(bool(reset))), "profile_read")
+        return {name: (p.ms[i], int(p.launches[i])) for i, name in enumerate(A.PROFILE_STAGES)}
+
+    def debug_links(self, surface: DeviceSurface, stream=None):
+        s = surface.c_struct()
+        n = C.c_int64()
+        L = A.load()
+        A.check(L.ffs_lbm_debug_links(self._h, C.byref(s), None, None, 0, C.byref(n), _stream_handle(stream)),
+                "debug_links")
+        cq = np.zeros(max(n.value, 1), dtype=np.uint64)
+        key = np.zeros(max(n.value, 1), dtype=np.uint64)
+        A.check(L.ffs_lbm_debug_links(self._h, C.byref(s), _np_ptr(cq), _np_ptr(key), n.value, C.byref(n),
+                                      _stream_handle(stream)), "debug_links")
+        return cq[: n.value], key[: n.value]

@@ -1,0 +1,48 @@
+"""The C-ABI library loads and exports exactly what include/ffs_lbm.h declares (no GPU)."""
+import ctypes
+import os
+import re
+
+from freeflow_b200 import _capi
+from freeflow_b200 import build as B
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_entry_points():
+    src = open(os.path.join(ROOT, "include", "ffs_lbm.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ffs_\w+)\s*\(", src)))
+
+
+def test_library_builds_and_loads():
+    path = B.build()
+    assert os.path.exists(path)
+    lib = ctypes.CDLL(path)
+    assert lib is not None
+
+
+def test_every_declared_symbol_is_exported():
+    lib = ctypes.CDLL(B.build())
+    names = declared_entry_points()
+    assert names, "no entry points found in the header"
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(_capi.EXPORTS) == names
+
+
+def test_abi_version_and_status_strings():
+    L = _capi.load()
+    assert L.ffs_abi_version() == 1
+    assert L.ffs_status_string(0) == b"ok"
+    assert L.ffs_status_string(1) == b"invalid argument"
+
+
+def test_invalid_descriptor_is_rejected_without_gpu_work():
+    L = _capi.load()
+    d = _capi.LbmDesc()
+    d.dim = 4
+    h = ctypes.c_void_p()
+    assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    assert b"dim" in L.ffs_last_error()
+    assert L.ffs_lbm_create(None, ctypes.byref(h)) == 1

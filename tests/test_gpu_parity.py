@@ -1,0 +1,170 @@
+"""GPU parity of the CUDA fluid step against the CPU oracle, through the C ABI.
+
+Tolerances (FP32 moments of a stable flow; the oracle and the kernels
+evaluate the same expressions in different FP32 operation orders, and the
+kernels contract into FMAs):
+  * moments, FP32 tile, vs the ref32 oracle ...... max |diff| <= 2e-6 after the steps run
+  * moments, binary16 D2Q9 tile (reference mode) .. rms <= 2e-5, max <= 1e-3 (a population
+    that lands on the other side of a binary16 rounding boundary moves by one half-ulp)
+  * link sets ...................................... identical (cell, direction, depth, element)
+  * surface forces (FP64 sums) ..................... max |diff| <= 1e-4 x max |F|
+"""
+import numpy as np
+import pytest
+
+from freeflow_b200 import workloads as W
+
+from helpers import make_gpu, make_oracle, max_abs, rms, run_pair
+
+pytestmark = pytest.mark.gpu
+
+
+def small_cylinder():
+    return W.cylinder_channel_2d(nx=64, ny=32, radius=6.0, center=(16.0, 16.0), nseg=48, seed=3)
+
+
+def small_swimmer_2d():
+    return W.swimmer_2d(nx=160, ny=64, body_frac=0.5, n_boundary=60, seed=4)
+
+
+def small_swimmer_3d():
+    return W.swimmer_3d(nx=64, ny=32, nz=32, body_frac=0.3, nlat=12, nlon=16, seed=5)
+
+
+# ------------------------------------------------------------------- D2Q9
+def test_2d_cylinder_fp32_matches_oracle(cuda):
+    gm, om, gf, of, st = run_pair(small_cylinder(), 12)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+    assert max_abs(gf, of) <= 1e-4 * max(np.abs(of).max(), 1e-30)
+
+
+def test_2d_cylinder_half_tile_matches_reference_mode(cuda):
+    gm, om, _, _, st = run_pair(small_cylinder(), 12, ref_half=True)
+    assert st == 0
+    assert rms(gm, om) <= 2e-5
+    assert max_abs(gm, om) <= 1e-3
+
+
+def test_2d_swimmer_moving_wall_and_forces(cuda):
+    gm, om, gf, of, st = run_pair(small_swimmer_2d(), 10)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+    assert np.abs(of).max() > 0
+    assert max_abs(gf, of) <= 1e-4 * np.abs(of).max()
+
+
+def test_2d_links_identical(cuda):
+    wl = small_swimmer_2d()
+    g, surf = make_gpu(wl)
+    o = make_oracle(wl)
+    v, u = wl.surface_at(7)
+    surf.update(v, u)
+    gcq, gkey = g.debug_links(surf)
+    o.step(v, u, wl.elements, None)
+    ocq, okey = o.links()
+    assert len(ocq) > 0
+    assert np.array_equal(gcq, ocq)
+    assert np.array_equal(gkey, okey)
+
+
+def test_2d_periodic_fp32_vs_fp64(cuda):
+    wl = W.cylinder_channel_2d(nx=48, ny=40, radius=5.0, center=(20.0, 20.0), nseg=40)
+    wl.flags[:] = W.FLUID
+    gm, om, _, _, st = run_pair(wl, 20, precision="phys64", periodic=3)
+    assert st == 0
+    assert max_abs(gm, om) <= 5e-6
+
+
+def test_2d_fill_solid_matches_oracle(cuda):
+    from freeflow_b200 import DeviceSurface
+
+    wl = small_cylinder()
+    g, surf = make_gpu(wl)
+    o = make_oracle(wl)
+    g.fill_solid(surf)
+    o.fill_solid(wl.rest, wl.elements)
+    gf, of = g.get_flags(), o.get_flags()
+    assert np.array_equal(gf, of)
+    assert (gf == W.SOLID_DYNAMIC).sum() > 0
+
+
+# ------------------------------------------------------------------ D3Q27
+def test_3d_swimmer_matches_oracle(cuda):
+    gm, om, gf, of, st = run_pair(small_swimmer_3d(), 6)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+    assert np.abs(of).max() > 0
+    assert max_abs(gf, of) <= 1e-4 * np.abs(of).max()
+
+
+def test_3d_links_identical(cuda):
+    wl = small_swimmer_3d()
+    g, surf = make_gpu(wl)
+    o = make_oracle(wl)
+    v, u = wl.surface_at(3)
+    surf.update(v, u)
+    gcq, gkey = g.debug_links(surf)
+    o.step(v, u, wl.elements, None)
+    ocq, okey = o.links()
+    assert len(ocq) > 0
+    assert np.array_equal(gcq, ocq)
+    assert np.array_equal(gkey, okey)
+
+
+def test_3d_taylor_green_periodic_vs_fp64(cuda):
+    wl = W.taylor_green_3d(n=32, u0=0.04, viscosity=0.005)
+    gm, om, _, _, st = run_pair(wl, 20, precision="phys64")
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+
+
+def test_3d_clamped_halo_reference_mode(cuda):
+    """Reference semantics without periodicity: the halo is clamped (quirk Q1)."""
+    wl = W.taylor_green_3d(n=20, u0=0.04, viscosity=0.01)
+    gm, om, _, _, st = run_pair(wl, 8, periodic=0)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+
+
+def test_3d_walls_inlet_outlet_channel(cuda):
+    wl = W.swimmer_3d(nx=40, ny=24, nz=24, nlat=8, nlon=12)
+    wl.elements = None
+    gm, om, _, _, st = run_pair(wl, 8)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+
+
+# ------------------------------------------------------- storage precision
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("bf16", 1e-2)])
+def test_reduced_storage_error_vs_fp64(cuda, storage, tol):
+    """Relative velocity error of FP16/BF16 scaled-moment storage against FP64."""
+    wl = W.taylor_green_3d(n=32, u0=0.04, viscosity=0.005)
+    gm, om, _, _, st = run_pair(wl, 50, storage=storage, precision="phys64")
+    assert st == 0
+    err = np.abs(gm[:, 1:4] - om[:, 1:4]).max() / np.abs(om[:, 1:4]).max()
+    assert err <= tol
+
+
+# ----------------------------------------------------------- status / faults
+def test_nonfinite_state_sets_status_without_fault(cuda):
+    """A poisoned moment (injected on the host) latches the non-finite bit."""
+    from freeflow_b200 import FluidGrid
+
+    wl = small_cylinder()
+    g = FluidGrid(**wl.grid_kwargs())
+    g.set_flags(wl.flags)
+    m = wl.moments.copy()
+    m[wl.nx * 10 + 20, 0] = np.nan
+    g.set_moments(m)
+    g.step()
+    assert g.status() & 1
+    assert g.status() == 0  # cleared by the previous read
+
+
+def test_deterministic_repeat(cuda):
+    wl = small_swimmer_3d()
+    a = run_pair(wl, 4)
+    b = run_pair(wl, 4)
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[2], b[2])
