@@ -39,6 +39,7 @@ struct ffs_lbm {
     Codec codec{};
     LinkTable lt;
     float *staging = nullptr; // ncell * NM floats, allocated on first host transfer
+    int dense_variant = -1;   // D3Q27 kernel variant chosen on the first step (tune_dense3d)
     // host-buffer step (ffs_lbm_step_host)
     float *hs_dev = nullptr;   // vertices | velocities | forces
     uint32_t *hs_elem = nullptr;
@@ -217,7 +218,10 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const ffs_surfac
     {
         StageTimer t(h, 1, st);
         if (DIM == 2) FFS_CK(launch_dense2d<T>(g, st));
-        else FFS_CK(launch_dense3d<T>(g, st));
+        else {
+            if (h->dense_variant < 0) h->dense_variant = tune_dense3d<T>(g, st);
+            FFS_CK(launch_dense3d<T>(g, st, h->dense_variant));
+        }
     }
     if (surf) {
         {

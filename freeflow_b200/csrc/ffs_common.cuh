@@ -105,6 +105,18 @@ enum StatusBits : uint32_t {
     kStatusBadElement = 1u << 3,    // element index out of range in the surface
 };
 
+// A post-collision state the step cannot continue from: density not
+// positive, or a non-finite density or velocity.  (Populations are clamped
+// with max(0, f) before the moments are formed, which turns a NaN population
+// into 0, so a poisoned neighbour shows up as a vanishing or infinite
+// density rather than as a NaN.)
+template <int DIM> __device__ __forceinline__ bool bad_state(const float *m)
+{
+    float s = m[0] + m[1] + m[2];
+    if (DIM == 3) s += m[3];
+    return !(m[0] > 0.0f) || !isfinite(s);
+}
+
 // ---------------------------------------------------------------- storage
 enum Storage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 
@@ -183,6 +195,29 @@ __device__ __forceinline__ void encode_store(const float *m, T *const *planes, u
 #pragma unroll
         for (int k = DIM + 1; k < NM; ++k)
             planes[k][idx] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+    }
+}
+
+// Same as encode_store with planes[k] = base + k * stride.
+template <int DIM, typename T>
+__device__ __forceinline__ void encode_store_strided(const float *m, T *base, size_t stride, const Codec &c)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    if constexpr (!StorageTraits<T>::kEncoded) {
+#pragma unroll
+        for (int k = 0; k < NM; ++k) base[k * stride] = StorageTraits<T>::to(m[k]);
+    } else {
+        float ud[DIM];
+        base[0] = StorageTraits<T>::to(m[0] - 1.0f);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            T s = StorageTraits<T>::to(m[1 + a] * c.su);
+            base[(1 + a) * stride] = s;
+            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
+        }
+#pragma unroll
+        for (int k = DIM + 1; k < NM; ++k)
+            base[k * stride] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
     }
 }
 

@@ -75,7 +75,7 @@ __device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y
 #pragma unroll
             for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
             encode_store<2, T>(m, planes, idx, g.codec);
-            if (!isfinite(m[0])) atomicOr(g.status, kStatusNonFinite);
+            if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
             if (f8 & kBitOutletSrc) feed_outlets<2, T>(g, idx);
         }
     }

@@ -7,11 +7,14 @@ namespace fflbm {
 struct D3 {
     static constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
     static constexpr int kHX = kTX + 2, kHY = kTY + 2, kHalo = kHX * kHY;
-    static constexpr int kSetFloats = 9 * kHalo; // one 9-population c_z slice of one plane
-    // one c_z=-1 slice, two c_z=0 slices, three c_z=+1 slices
-    static constexpr size_t kSmemBytes = 6 * (size_t)kSetFloats * sizeof(float);
+    static constexpr int kHalf = kHalo / 2;                   // halo cells per reconstructing thread pair
+    static constexpr int kPlaneFloats = 27 * kHalo;           // all populations of one halo plane
+    static constexpr size_t kSmemBytes = 2 * (size_t)kPlaneFloats * sizeof(float); // double buffer
 };
+static_assert(D3::kHalo % 2 == 0, "halo plane must split into pairs");
 
-template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s);
+// variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM
+template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant);
+template <typename T> int tune_dense3d(const GridArgs<T> &g, cudaStream_t s);
 
 } // namespace fflbm

@@ -126,6 +126,61 @@ __device__ __forceinline__ Hit isect3(const float *V, uint32_t ia, uint32_t ib, 
     return r;
 }
 
+// Per-triangle part of isect3: everything that depends only on the
+// triangle, evaluated with exactly the same operations, so isect3_pre()
+// returns bit-identical results to isect3() while doing it once per triangle.
+struct TriPre {
+    float v0[3], e1[3], e2[3], n[3];
+    float d00, d01, d11, den;
+};
+
+__device__ __forceinline__ TriPre tri_pre(const float *V, uint32_t ia, uint32_t ib, uint32_t ic)
+{
+    TriPre t;
+    float v1[3], v2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { t.v0[k] = V[3 * (size_t)ia + k]; v1[k] = V[3 * (size_t)ib + k]; v2[k] = V[3 * (size_t)ic + k]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { t.e1[k] = sub(v1[k], t.v0[k]); t.e2[k] = sub(v2[k], t.v0[k]); }
+    cross3(t.e1, t.e2, t.n);
+    normalize3(t.n);
+    t.d00 = dot3(t.e1, t.e1);
+    t.d01 = dot3(t.e1, t.e2);
+    t.d11 = dot3(t.e2, t.e2);
+    t.den = sub(mul(t.d00, t.d11), mul(t.d01, t.d01));
+    return t;
+}
+
+__device__ __forceinline__ Hit isect3_pre(const TriPre &tr, const float *p1, const float *p2)
+{
+    Hit r;
+    r.hit = false; r.depth = 0.0f; r.b[0] = r.b[1] = r.b[2] = 0.0f;
+    float d[3], w0[3], pd[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = sub(p2[k], p1[k]);
+    normalize3(d);
+    float nd = dot3(tr.n, d);
+    if (fabsf(nd) <= 1e-6f) return r;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { w0[k] = sub(tr.v0[k], p1[k]); pd[k] = sub(p2[k], p1[k]); }
+    float t = dvd(dot3(tr.n, w0), dot3(tr.n, pd));
+    if (t < 0.0f || t > 1.0f) return r;
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) w[k] = sub(add(p1[k], mul(t, pd[k])), tr.v0[k]);
+    float d20 = dot3(w, tr.e1), d21 = dot3(w, tr.e2);
+    float u0 = dvd(sub(mul(tr.d11, d20), mul(tr.d01, d21)), tr.den);
+    float vv = dvd(sub(mul(tr.d00, d21), mul(tr.d01, d20)), tr.den);
+    if (u0 >= -1e-6f && vv >= -1e-6f && add(u0, vv) <= 1.0f + 1e-6f) {
+        r.hit = true;
+        r.depth = t;
+        r.b[0] = sub(sub(1.0f, u0), vv);
+        r.b[1] = u0;
+        r.b[2] = vv;
+    }
+    return r;
+}
+
 // depthIndexCompact widened to 64 bits: (uint32(depth * 2^15) << 32) | element.
 // Orders exactly like the reference's 32-bit key for up to 65536 elements.
 __device__ __forceinline__ unsigned long long link_key(float depth, uint32_t e)

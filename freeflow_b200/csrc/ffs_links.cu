@@ -65,6 +65,120 @@ __device__ __forceinline__ void set_link_bit(uint32_t *flag_words, uint32_t cell
 }
 
 // ------------------------------------------------------------------ detect
+static int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+// Finds or claims the cell's slot and keeps the smallest key of direction l.
+template <int Q>
+__device__ __forceinline__ void insert_link(const LinkTable &lt, uint32_t *flag_words, uint32_t cell, int l,
+                                            unsigned long long key, uint32_t *status)
+{
+    uint32_t slot = hash_cell(cell) & (lt.cap - 1);
+    for (uint32_t probe = 0; probe < lt.cap; ++probe) {
+        uint32_t cur = lt.keys[slot];
+        if (cur == 0) {
+            uint32_t old = atomicCAS(lt.keys + slot, 0u, cell + 1);
+            if (old == 0) {
+                uint32_t pos = atomicAdd(lt.count, 1u);
+                lt.list[pos] = slot;
+                set_link_bit(flag_words, cell, true);
+                cur = cell + 1;
+            } else {
+                cur = old;
+            }
+        }
+        if (cur == cell + 1) {
+            atomicMin(lt.links + (size_t)slot * Q + l, key);
+            return;
+        }
+        slot = (slot + 1) & (lt.cap - 1);
+    }
+    atomicOr(status, kStatusLinkOverflow);
+}
+
+// D3Q27: one warp per triangle.  The triangle's own geometry is evaluated
+// once (tri_pre); lanes stride over (bounding-box cell, direction) pairs.  A
+// conservative plane-distance test discards the pairs whose link segment
+// clearly does not reach the triangle's plane (|signed distance of the cell|
+// > |projection of the link| + a margin of 2e-3 cells, far above the float
+// rounding of either quantity); every remaining pair gets the exact test.
+template <typename T>
+__global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt,
+                                                            SurfaceArgs s, StepScalars sc)
+{
+    constexpr int Q = 27;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const float cl = sc.cl;
+    const float margin = 2e-3f * cl;
+    for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < s.ne; e += nwarps) {
+        const uint32_t ia = s.E[3 * e], ib = s.E[3 * e + 1], ic = s.E[3 * e + 2];
+        if (ia >= (uint32_t)s.nv || ib >= (uint32_t)s.nv || ic >= (uint32_t)s.nv) {
+            if (lane == 0) atomicOr(g.status, kStatusBadElement);
+            continue;
+        }
+        const geom::TriPre tr = geom::tri_pre(s.V, ia, ib, ic);
+        float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+        float bmax[3] = {1.175494351e-38f, 1.175494351e-38f, 1.175494351e-38f};
+        const uint32_t vid[3] = {ia, ib, ic};
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float c = s.V[(size_t)vid[j] * 3 + k];
+                if (c < bmin[k]) bmin[k] = c;
+                if (bmax[k] < c) bmax[k] = c;
+            }
+        const int n3[3] = {g.nx, g.ny, g.nz};
+        int lo[3], ext[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = max(__float2int_rz(geom::dvd(bmin[k], cl)) - 1, 0);
+            int hi = min(__float2int_rz(geom::dvd(bmax[k], cl)) + 1, n3[k] - 1);
+            ext[k] = max(hi - lo[k] + 1, 0);
+        }
+        const int ncells = ext[0] * ext[1] * ext[2];
+        const int items = ncells * (Q - 1);
+        for (int it = lane; it < items; it += 32) {
+            const int l = it % (Q - 1) + 1;
+            const int c = it / (Q - 1);
+            const int i = lo[0] + c % ext[0];
+            const int j = lo[1] + (c / ext[0]) % ext[1];
+            const int k3 = lo[2] + c / (ext[0] * ext[1]);
+            int cx, cy, cz;
+            dir_vec<3>(l, cx, cy, cz);
+            // prefilter (ordinary float math; only ever rejects clear misses)
+            const float s1 = tr.n[0] * ((float)i * cl - tr.v0[0]) + tr.n[1] * ((float)j * cl - tr.v0[1]) +
+                             tr.n[2] * ((float)k3 * cl - tr.v0[2]);
+            const float a = cl * (tr.n[0] * cx + tr.n[1] * cy + tr.n[2] * cz);
+            // exact t = s1 / a (approximately); a miss needs t < 0 or t > 1
+            if (fabsf(a) > margin) {
+                const float t = s1 / a;
+                const float tol = margin / fabsf(a);
+                if (t < -tol || t > 1.0f + tol) continue;
+            } else if (fabsf(s1) > 2.0f * margin) {
+                continue; // link parallel to the plane and away from it
+            }
+            float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
+            float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl), geom::mul(geom::sub((float)j, (float)cy), cl),
+                           geom::mul(geom::sub((float)k3, (float)cz), cl)};
+            const geom::Hit h = geom::isect3_pre(tr, p1, p2);
+            if (!h.hit) continue;
+            const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
+            insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status);
+        }
+    }
+}
+
 template <int DIM, typename T>
 __global__ void detect_links_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s, StepScalars sc)
 {
@@ -117,28 +231,7 @@ __global__ void detect_links_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTab
                 }
                 if (!h.hit) continue;
                 const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
-                const unsigned long long key = geom::link_key(h.depth, (uint32_t)e);
-                // find or claim the cell's slot
-                uint32_t slot = hash_cell(cell) & (lt.cap - 1);
-                bool ok = false;
-                for (uint32_t probe = 0; probe < lt.cap; ++probe) {
-                    uint32_t cur = lt.keys[slot];
-                    if (cur == cell + 1) { ok = true; break; }
-                    if (cur == 0) {
-                        uint32_t old = atomicCAS(lt.keys + slot, 0u, cell + 1);
-                        if (old == 0) {
-                            uint32_t pos = atomicAdd(lt.count, 1u);
-                            lt.list[pos] = slot;
-                            set_link_bit(flag_words, cell, true);
-                            ok = true;
-                            break;
-                        }
-                        if (old == cell + 1) { ok = true; break; }
-                    }
-                    slot = (slot + 1) & (lt.cap - 1);
-                }
-                if (!ok) { atomicOr(g.status, kStatusLinkOverflow); continue; }
-                atomicMin(lt.links + (size_t)slot * Q + l, key);
+                insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status);
             }
 }
 
@@ -336,7 +429,7 @@ __global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t
 #pragma unroll
                 for (int k = 0; k < NM; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
                 encode_store<DIM, T>(m, planes, cell, g.codec);
-                if (!isfinite(m[0])) atomicOr(g.status, kStatusNonFinite);
+                if (bad_state<DIM>(m)) atomicOr(g.status, kStatusNonFinite);
                 if (f8 & kBitOutletSrc) feed_outlets<DIM, T>(g, cell);
             }
         }
@@ -383,25 +476,19 @@ __global__ void reset_links_kernel(LinkTable lt, uint32_t *flag_words)
 __global__ void zero_count_kernel(uint32_t *count) { *count = 0; }
 
 // ---------------------------------------------------------------- launchers
-static int sm_count()
-{
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
-
 template <int DIM, typename T>
 cudaError_t launch_detect_links(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
                                 const StepScalars &sc, cudaStream_t st)
 {
     constexpr int Q = Lattice<DIM>::Q;
+    if (s.ne <= 0) return cudaSuccess;
+    if (DIM == 3) {
+        long long warps = s.ne;
+        int grid = (int)std::min<long long>((warps + 7) / 8, (long long)sm_count() * 16);
+        detect_links3_kernel<T><<<grid, 256, 0, st>>>(g, flag_words, lt, s, sc);
+        return cudaGetLastError();
+    }
     long long threads = (long long)s.ne * (Q - 1);
-    if (threads <= 0) return cudaSuccess;
     int block = 128;
     long long grid = (threads + block - 1) / block;
     detect_links_kernel<DIM, T><<<(unsigned)grid, block, 0, st>>>(g, flag_words, lt, s, sc);

@@ -16,6 +16,7 @@
 // the reference's up to FP32 rounding order.
 #pragma once
 #include "ffs_common.cuh"
+#include "ffs_f2.cuh"
 
 namespace fflbm {
 
@@ -164,6 +165,101 @@ template <> struct Coef<3> {
         s = fmaf(qxyz, fx * fy * fz, s);
         float w = (cx ? 1.0f / 6.0f : 2.0f / 3.0f) * (cy ? 1.0f / 6.0f : 2.0f / 3.0f) * (cz ? 1.0f / 6.0f : 2.0f / 3.0f);
         return w * s;
+    }
+};
+
+// D3Q27 reconstruction generic in the arithmetic type: V = float (one cell)
+// or V = f2 (two cells per thread, packed FP32 pairs).
+template <typename V> __device__ __forceinline__ void herm3v(V a0, V a1, V a2, V *v)
+{
+    V t = a0 + a2;
+    v[0] = t - a1;
+    v[1] = vfma(vconst<V>(-0.5f), a2, a0);
+    v[2] = t + a1;
+}
+template <typename V> __device__ __forceinline__ void herm2v(V a0, V a1, V *v)
+{
+    v[0] = a0 - a1;
+    v[1] = a0;
+    v[2] = a0 + a1;
+}
+
+template <typename V> struct Coef3V {
+    V rho, m1x, m1y, m1z, m2xx, m2yy, m2zz, m2xy, m2yz, m2xz;
+    V qxxy, qxyy, qxxz, qxzz, qyyz, qyzz, qxyz;
+    // same expressions as Coef<3>::make
+    __device__ __forceinline__ void make(const V *m)
+    {
+        V r = m[0], ux = m[1], uy = m[2], uz = m[3];
+        V pxx = m[4], pyy = m[5], pzz = m[6], pxy = m[7], pyz = m[8], pxz = m[9];
+        V r3 = vconst<V>(3.0f) * r, r9 = vconst<V>(9.0f) * r;
+        rho = r;
+        m1x = r3 * ux; m1y = r3 * uy; m1z = r3 * uz;
+        m2xx = r3 * pxx; m2yy = r3 * pyy; m2zz = r3 * pzz;
+        m2xy = r9 * pxy; m2yz = r9 * pyz; m2xz = r9 * pxz;
+        V zero = vconst<V>(0.0f);
+        V dxy = vfma(zero - ux, uy, pxy), dyz = vfma(zero - uy, uz, pyz), dxz = vfma(zero - ux, uz, pxz);
+        V r18 = vconst<V>(2.0f) * r9;
+        qxxy = vfma(r9 * pxx, uy, r18 * ux * dxy);
+        qxyy = vfma(r9 * pyy, ux, r18 * uy * dxy);
+        qxxz = vfma(r9 * pxx, uz, r18 * ux * dxz);
+        qxzz = vfma(r9 * pzz, ux, r18 * uz * dxz);
+        qyyz = vfma(r9 * pyy, uz, r18 * uy * dyz);
+        qyzz = vfma(r9 * pzz, uy, r18 * uz * dyz);
+        V t = vfma(pxy, uz, vfma(pyz, ux, pxz * uy));
+        qxyz = vconst<V>(27.0f) * r * vfma(vconst<V>(-2.0f) * ux * uy, uz, t);
+    }
+    // Evaluates the 27 populations slice by slice and hands each one to
+    // sink(kz, ky, kx, value) as soon as it exists (k = c + 1), which keeps
+    // register pressure low when the sink stores to shared memory.
+    template <typename Sink> __device__ __forceinline__ void populations_each(Sink &&sink) const
+    {
+        V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
+        herm3v(rho, m1z, m2zz, B00);
+        herm3v(m1x, m2xz, qxzz, B10);
+        herm3v(m1y, m2yz, qyzz, B01);
+        herm2v(m2xx, qxxz, B20);
+        herm2v(m2yy, qyyz, B02);
+        herm2v(m2xy, qxyz, B11);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            V C0[3], C1[3], C2[3];
+            herm3v(B00[kz], B01[kz], B02[kz], C0);
+            herm3v(B10[kz], B11[kz], qxyy, C1);
+            herm2v(B20[kz], qxxy, C2);
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                V F[3];
+                herm3v(C0[ky], C1[ky], C2[ky], F);
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) sink(kz, ky, kx, vconst<V>(wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx]);
+            }
+        }
+    }
+    // out[kz][ky][kx], k = c + 1
+    __device__ __forceinline__ void populations_xyz(V (*out)[3][3]) const
+    {
+        V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
+        herm3v(rho, m1z, m2zz, B00);
+        herm3v(m1x, m2xz, qxzz, B10);
+        herm3v(m1y, m2yz, qyzz, B01);
+        herm2v(m2xx, qxxz, B20);
+        herm2v(m2yy, qyyz, B02);
+        herm2v(m2xy, qxyz, B11);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            V C0[3], C1[3], C2[3];
+            herm3v(B00[kz], B01[kz], B02[kz], C0);
+            herm3v(B10[kz], B11[kz], qxyy, C1);
+            herm2v(B20[kz], qxxy, C2);
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                V F[3];
+                herm3v(C0[ky], C1[ky], C2[ky], F);
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = vconst<V>(wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx];
+            }
+        }
     }
 };
 

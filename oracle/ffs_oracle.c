@@ -23,6 +23,88 @@ enum {
     FL_OUT_L = 19, FL_OUT_R = 20, FL_OUT_U = 21, FL_OUT_D = 22, FL_OUT_F = 23, FL_OUT_B = 24
 };
 
+/* ---------------------------------------------------------------- geometry
+ * FP32 restatement of the link geometry (SolidGeometryProxy_Device.cuh):
+ * line_intersect :89-124, 2D intersectAtIndex :211-227, glm dot/cross/
+ * normalize, barycentric_coordinates :291-304, line_triangle_intersect
+ * :306-341 with the NumericUtils tolerance 1e-6 (NumericUtils.cuh:24).
+ * Built with -ffp-contract=off: each operation rounds once, in order. */
+typedef struct { int hit; float depth; float b[3]; } geo_hit;
+
+static float geo_line(float x1, float y1, float x2, float y2, float x3, float y3, float x4, float y4, float *xo, float *yo)
+{
+    float a1 = (x1 - x2) * (y3 - y4) - (y1 - y2) * (x3 - x4);
+    float b1 = (x4 - x2) * (y3 - y4) - (y4 - y2) * (x3 - x4);
+    if (fabsf(a1) <= 0.0f) return -1.0f;
+    float t1 = b1 / a1;
+    if (t1 <= 0.0f || t1 >= 1.0f) return -1.0f;
+    *xo = t1 * x1 + (1.0f - t1) * x2;
+    if ((x3 - *xo) * (x4 - *xo) < 0.0f) {
+        *yo = t1 * y1 + (1.0f - t1) * y2;
+        return 1.0f - t1;
+    }
+    return -1.0f;
+}
+
+static geo_hit geo_isect2(const float *V, const uint32_t *E, int e, float p1x, float p1y, float p2x, float p2y)
+{
+    geo_hit r = {0, 0.0f, {0.0f, 0.0f, 0.0f}};
+    uint32_t s = E[2 * e], t = E[2 * e + 1];
+    float x3 = V[2 * s], y3 = V[2 * s + 1], x4 = V[2 * t], y4 = V[2 * t + 1];
+    float xo = 0.0f, yo = 0.0f;
+    float d = geo_line(p1x, p1y, p2x, p2y, x3, y3, x4, y4, &xo, &yo);
+    if (d > 0.0f && d < 1.0f) {
+        float dxh = x4 - xo, dyh = y4 - yo, dx34 = x4 - x3, dy34 = y4 - y3;
+        float l1 = sqrtf(dxh * dxh + dyh * dyh);
+        float l2 = sqrtf(dx34 * dx34 + dy34 * dy34);
+        r.hit = 1; r.depth = d; r.b[0] = l1 / l2; r.b[1] = 1.0f - r.b[0];
+    }
+    return r;
+}
+
+static inline float geo_dot(const float *a, const float *b) { float x = a[0] * b[0], y = a[1] * b[1], z = a[2] * b[2]; return x + y + z; }
+static inline void geo_cross(const float *a, const float *b, float *o)
+{
+    o[0] = a[1] * b[2] - b[1] * a[2];
+    o[1] = a[2] * b[0] - b[2] * a[0];
+    o[2] = a[0] * b[1] - b[0] * a[1];
+}
+static inline void geo_normalize(float *v)
+{
+    float inv = 1.0f / sqrtf(geo_dot(v, v));
+    v[0] = v[0] * inv; v[1] = v[1] * inv; v[2] = v[2] * inv;
+}
+
+static geo_hit geo_isect3(const float *V, const uint32_t *E, int e, const float *p1, const float *p2)
+{
+    geo_hit r = {0, 0.0f, {0.0f, 0.0f, 0.0f}};
+    float v[3][3];
+    for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) v[j][k] = V[(size_t)E[3 * e + j] * 3 + k];
+    float e1[3], e2[3], n[3], d[3], w0[3], pd[3];
+    for (int k = 0; k < 3; ++k) { e1[k] = v[1][k] - v[0][k]; e2[k] = v[2][k] - v[0][k]; }
+    geo_cross(e1, e2, n);
+    geo_normalize(n);
+    for (int k = 0; k < 3; ++k) d[k] = p2[k] - p1[k];
+    geo_normalize(d);
+    if (fabsf(geo_dot(n, d)) <= 1e-6f) return r;
+    for (int k = 0; k < 3; ++k) { w0[k] = v[0][k] - p1[k]; pd[k] = p2[k] - p1[k]; }
+    float t = geo_dot(n, w0) / geo_dot(n, pd);
+    if (t < 0.0f || t > 1.0f) return r;
+    float w[3];
+    for (int k = 0; k < 3; ++k) w[k] = (p1[k] + t * pd[k]) - v[0][k];
+    float d00 = geo_dot(e1, e1), d01 = geo_dot(e1, e2), d11 = geo_dot(e2, e2);
+    float d20 = geo_dot(w, e1), d21 = geo_dot(w, e2);
+    float den = d00 * d11 - d01 * d01;
+    float u0 = (d11 * d20 - d01 * d21) / den;
+    float v0 = (d00 * d21 - d01 * d20) / den;
+    const float one_eps = 1.0f + 1e-6f;
+    if (u0 >= -1e-6f && v0 >= -1e-6f && u0 + v0 <= one_eps) {
+        r.hit = 1; r.depth = t; r.b[0] = (1.0f - u0) - v0; r.b[1] = u0; r.b[2] = v0;
+    }
+    return r;
+}
+
 #define R float
 #define FN(x) ffo32_##x
 #include "ffs_oracle_impl.h"

@@ -47,6 +47,7 @@ typedef struct {
     int periodic;   /* bit0 x, bit1 y, bit2 z: halo wraps instead of clamping */
     int half_pops;  /* D2Q9: round the reconstructed tile to binary16 (reference smem) */
     R vis, cl, ct, cf, omega;
+    float clf;      /* lattice spacing as the reference's float (link geometry) */
     float bcvel[6];
     uint8_t *flags;
     R *mom[2];      /* AoS, NM values per cell, like the reference */
@@ -318,103 +319,32 @@ static inline R FN(round_pop)(const FN(grid) *g, R v)
 }
 
 /* ----------------------------------------------------------------- geometry
- * Restated from SolidGeometryProxy_Device.cuh.  Compiled with
- * -ffp-contract=off so every operation rounds once, in the written order;
- * the CUDA path writes the same operations with explicit __f*_rn intrinsics,
- * so both sides find identical link sets. */
+ * Restated from SolidGeometryProxy_Device.cuh in ffs_oracle.c (geo_* below),
+ * in FP32 for BOTH builds: the surface arrays are FP32 in the reference and
+ * the link set is a discrete function of them, so the FP64 build uses the very
+ * same links and differs from the FP32 build only in the fluid arithmetic. */
 
 typedef struct { int hit; R depth; R b[3]; } FN(isect);
 
-/* line_intersect, SolidGeometryProxy_Device.cuh:89-124 */
-static R FN(line_isect)(R x1, R y1, R x2, R y2, R x3, R y3, R x4, R y4, R *xo, R *yo)
-{
-    R a1 = (x1 - x2) * (y3 - y4) - (y1 - y2) * (x3 - x4);
-    R b1 = (x4 - x2) * (y3 - y4) - (y4 - y2) * (x3 - x4);
-    if (fabs((double)a1) <= 0.0) return (R)-1;
-    R t1 = b1 / a1;
-    if (t1 <= 0 || t1 >= 1) return (R)-1;
-    *xo = t1 * x1 + ((R)1 - t1) * x2;
-    if ((x3 - *xo) * (x4 - *xo) < 0) {
-        *yo = t1 * y1 + ((R)1 - t1) * y2;
-        return (R)1 - t1;
-    }
-    return (R)-1;
-}
-
-/* intersectAtIndex (2D), :211-227 */
 static FN(isect) FN(isect2)(const float *V, const uint32_t *E, int e, R p1x, R p1y, R p2x, R p2y)
 {
-    FN(isect) r; r.hit = 0; r.depth = 0; r.b[0] = r.b[1] = r.b[2] = 0;
-    uint32_t s = E[2 * e], t = E[2 * e + 1];
-    R x3 = V[2 * s], y3 = V[2 * s + 1], x4 = V[2 * t], y4 = V[2 * t + 1];
-    R xo = 0, yo = 0;
-    R d = FN(line_isect)(p1x, p1y, p2x, p2y, x3, y3, x4, y4, &xo, &yo);
-    if (d > 0 && d < 1) {
-        R dxh = x4 - xo, dyh = y4 - yo, dx34 = x4 - x3, dy34 = y4 - y3;
-        R l1 = (R)sqrt((double)(dxh * dxh + dyh * dyh));
-        R l2 = (R)sqrt((double)(dx34 * dx34 + dy34 * dy34));
-        if (sizeof(R) == 4) { l1 = sqrtf((float)(dxh * dxh + dyh * dyh)); l2 = sqrtf((float)(dx34 * dx34 + dy34 * dy34)); }
-        r.hit = 1; r.depth = d;
-        r.b[0] = l1 / l2;
-        r.b[1] = (R)1 - r.b[0];
-    }
+    geo_hit h = geo_isect2(V, E, e, (float)p1x, (float)p1y, (float)p2x, (float)p2y);
+    FN(isect) r; r.hit = h.hit; r.depth = (R)h.depth; r.b[0] = (R)h.b[0]; r.b[1] = (R)h.b[1]; r.b[2] = (R)h.b[2];
     return r;
 }
 
-static inline R FN(dot3)(const R *a, const R *b) { R x = a[0] * b[0], y = a[1] * b[1], z = a[2] * b[2]; return x + y + z; }
-static inline void FN(cross3)(const R *a, const R *b, R *o)
-{
-    o[0] = a[1] * b[2] - b[1] * a[2];
-    o[1] = a[2] * b[0] - b[2] * a[0];
-    o[2] = a[0] * b[1] - b[0] * a[1];
-}
-static inline void FN(normalize3)(R *v)
-{
-    R d = FN(dot3)(v, v);
-    R s = (sizeof(R) == 4) ? (R)sqrtf((float)d) : (R)sqrt((double)d);
-    R inv = (R)1 / s;
-    v[0] = v[0] * inv; v[1] = v[1] * inv; v[2] = v[2] * inv;
-}
-
-#define FN_EPS ((R)1e-6f)
-
-/* line_triangle_intersect + barycentric_coordinates, :291-341 */
 static FN(isect) FN(isect3)(const float *V, const uint32_t *E, int e, const R *p1, const R *p2)
 {
-    FN(isect) r; r.hit = 0; r.depth = 0; r.b[0] = r.b[1] = r.b[2] = 0;
-    R v[3][3];
-    for (int j = 0; j < 3; ++j)
-        for (int k = 0; k < 3; ++k) v[j][k] = V[(size_t)E[3 * e + j] * 3 + k];
-    R e1[3], e2[3], n[3], d[3], w0[3], pd[3];
-    for (int k = 0; k < 3; ++k) { e1[k] = v[1][k] - v[0][k]; e2[k] = v[2][k] - v[0][k]; }
-    FN(cross3)(e1, e2, n);
-    FN(normalize3)(n);
-    for (int k = 0; k < 3; ++k) d[k] = p2[k] - p1[k];
-    FN(normalize3)(d);
-    R nd = FN(dot3)(n, d);
-    if ((nd < 0 ? -nd : nd) <= FN_EPS) return r;
-    for (int k = 0; k < 3; ++k) { w0[k] = v[0][k] - p1[k]; pd[k] = p2[k] - p1[k]; }
-    R t = FN(dot3)(n, w0) / FN(dot3)(n, pd);
-    if (t < 0 || t > 1) return r;
-    R ip[3], w[3];
-    for (int k = 0; k < 3; ++k) ip[k] = p1[k] + t * pd[k];
-    for (int k = 0; k < 3; ++k) w[k] = ip[k] - v[0][k];
-    R d00 = FN(dot3)(e1, e1), d01 = FN(dot3)(e1, e2), d11 = FN(dot3)(e2, e2);
-    R d20 = FN(dot3)(w, e1), d21 = FN(dot3)(w, e2);
-    R den = d00 * d11 - d01 * d01;
-    R u0 = (d11 * d20 - d01 * d21) / den;
-    R v0 = (d00 * d21 - d01 * d20) / den;
-    if (u0 >= (R)0 - FN_EPS && v0 >= (R)0 - FN_EPS && u0 + v0 <= (R)1 + FN_EPS) {
-        r.hit = 1; r.depth = t;
-        r.b[0] = (R)1 - u0 - v0; r.b[1] = u0; r.b[2] = v0;
-    }
+    float a[3] = {(float)p1[0], (float)p1[1], (float)p1[2]}, b[3] = {(float)p2[0], (float)p2[1], (float)p2[2]};
+    geo_hit h = geo_isect3(V, E, e, a, b);
+    FN(isect) r; r.hit = h.hit; r.depth = (R)h.depth; r.b[0] = (R)h.b[0]; r.b[1] = (R)h.b[1]; r.b[2] = (R)h.b[2];
     return r;
 }
 
 /* depthIndexCompact, :79-85, widened to 64 bits (see file header). */
 static inline uint64_t FN(link_key)(R depth, int e)
 {
-    uint32_t dq = (uint32_t)(depth * (R)32768);
+    uint32_t dq = (uint32_t)((float)depth * 32768.0f);
     return ((uint64_t)dq << 32) | (uint32_t)e;
 }
 
@@ -469,6 +399,7 @@ FN(grid) *FN(create)(int dim, int nx, int ny, int nz, double viscosity, double d
     g->vis = (R)visf;
     g->omega = (sizeof(R) == 4) ? (R)(1.0 / ((double)visf * 3.0 + 0.5)) : (R)(1.0 / (viscosity * 3.0 + 0.5));
     g->cl = (sizeof(R) == 4) ? (R)(float)dx : (R)dx;
+    g->clf = (float)dx;
     g->ct = (sizeof(R) == 4) ? (R)(float)dt : (R)dt;
     /* getCf, Config.hpp:96-100 (2D) and :154-158 (3D) */
     if (sizeof(R) == 4) {
@@ -680,11 +611,12 @@ static void FN(update_cell)(FN(grid) *g, const R *src, R *dst, int x, int y, int
             if (li >= 0) {
                 int e = (int)(g->link_key[li] & 0xFFFFFFFFu);
                 FN(isect) in;
+                const float cl = g->clf;
                 if (dim == 2) {
-                    in = FN(isect2)(S->V, S->E, e, (R)x * g->cl, (R)y * g->cl, (R)x1 * g->cl, (R)y1 * g->cl);
+                    in = FN(isect2)(S->V, S->E, e, (float)x * cl, (float)y * cl, (float)x1 * cl, (float)y1 * cl);
                 } else {
-                    R p1[3] = {(R)x * g->cl, (R)y * g->cl, (R)z * g->cl};
-                    R p2[3] = {(R)x1 * g->cl, (R)y1 * g->cl, (R)z1 * g->cl};
+                    R p1[3] = {(float)x * cl, (float)y * cl, (float)z * cl};
+                    R p2[3] = {(float)x1 * cl, (float)y1 * cl, (float)z1 * cl};
                     in = FN(isect3)(S->V, S->E, e, p1, p2);
                 }
                 if (in.hit) {
@@ -816,19 +748,19 @@ static void FN(build_links)(FN(grid) *g, const FN(surface) *S)
     FN(cand) *cand = (FN(cand) *)malloc(sizeof(FN(cand)) * capc);
     for (int e = 0; e < S->ne; ++e) {
         /* getBoundingBox: min starts at FLT_MAX, max at FLT_MIN (:198-209, :424-440) */
-        R bmin[3] = {(R)FLT_MAX, (R)FLT_MAX, (R)FLT_MAX}, bmax[3] = {(R)FLT_MIN, (R)FLT_MIN, (R)FLT_MIN};
+        float bmin[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bmax[3] = {FLT_MIN, FLT_MIN, FLT_MIN};
         for (int j = 0; j < dim; ++j) {
             uint32_t v = S->E[dim * e + j];
             for (int k = 0; k < dim; ++k) {
-                R c = (R)S->V[(size_t)v * dim + k];
+                float c = S->V[(size_t)v * dim + k];
                 if (c < bmin[k]) bmin[k] = c;
                 if (bmax[k] < c) bmax[k] = c;
             }
         }
         int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         for (int k = 0; k < dim; ++k) {
-            lo[k] = (int)(bmin[k] / g->cl) - 1;
-            hi[k] = (int)(bmax[k] / g->cl) + 1;
+            lo[k] = (int)(bmin[k] / g->clf) - 1;
+            hi[k] = (int)(bmax[k] / g->clf) + 1;
         }
         for (int l = 1; l < Q; ++l) {
             for (int k3 = (dim == 3 ? lo[2] : 0); k3 <= (dim == 3 ? hi[2] : 0); ++k3) {
@@ -838,12 +770,13 @@ static void FN(build_links)(FN(grid) *g, const FN(surface) *S)
                     for (int i = lo[0]; i <= hi[0]; ++i) {
                         if (i < 0 || i >= nx) continue;
                         FN(isect) in;
+                        const float cl = g->clf;
                         if (dim == 2) {
-                            in = FN(isect2)(S->V, S->E, e, (R)i * g->cl, (R)j * g->cl,
-                                            ((R)i - (R)ex[l]) * g->cl, ((R)j - (R)ey[l]) * g->cl);
+                            in = FN(isect2)(S->V, S->E, e, (float)i * cl, (float)j * cl,
+                                            ((float)i - (float)ex[l]) * cl, ((float)j - (float)ey[l]) * cl);
                         } else {
-                            R p1[3] = {(R)i * g->cl, (R)j * g->cl, (R)k3 * g->cl};
-                            R p2[3] = {((R)i - (R)ex[l]) * g->cl, ((R)j - (R)ey[l]) * g->cl, ((R)k3 - (R)ez[l]) * g->cl};
+                            R p1[3] = {(float)i * cl, (float)j * cl, (float)k3 * cl};
+                            R p2[3] = {((float)i - (float)ex[l]) * cl, ((float)j - (float)ey[l]) * cl, ((float)k3 - (float)ez[l]) * cl};
                             in = FN(isect3)(S->V, S->E, e, p1, p2);
                         }
                         if (!in.hit) continue;
@@ -980,11 +913,11 @@ void FN(fill_solid2)(FN(grid) *g, const float *V, const uint32_t *E, int ne)
         for (int x = 0; x < g->nx; ++x) {
             long long c = (long long)y * g->nx + x;
             if (g->flags[c] != FL_FLUID) continue;
-            R px = ((R)x + (R)0.5) * g->cl, py = ((R)y + (R)0.5) * g->cl;
+            float px = ((float)x + 0.5f) * g->clf, py = ((float)y + 0.5f) * g->clf;
             int in = 0;
             for (int i = 0; i < ne; ++i) {
                 uint32_t a = E[2 * i], b = E[2 * i + 1];
-                R sx = V[2 * a], sy = V[2 * a + 1], tx = V[2 * b], ty = V[2 * b + 1];
+                float sx = V[2 * a], sy = V[2 * a + 1], tx = V[2 * b], ty = V[2 * b + 1];
                 if ((sy < py && ty >= py) || (sy >= py && ty < py))
                     in ^= (sx + (py - sy) * (tx - sx) / (ty - sy) > px);
             }
