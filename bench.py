@@ -218,6 +218,7 @@ def run_ours(args):
     g.set_moments(wl.moments)
     stream = torch.cuda.Stream()
     surf = None
+    link_stats = None
     nsteps_total = K + Wm
     if wl.elements is not None:
         v0, u0 = wl.surface_at(0)
@@ -230,6 +231,8 @@ def run_ours(args):
             V[s], U[s] = wl.surface_at(s)
         Vd = torch.from_numpy(V).cuda()
         Ud = torch.from_numpy(U).cuda()
+        cq, _ = g.debug_links(surf)
+        link_stats = {"links": int(cq.size), "link_cells": int(np.unique(cq // g.info.q).size)}
 
     def step(s):
         if surf is not None:
@@ -339,6 +342,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": storage, "data": "synthetic (seeded)",
             "config": {"workload": wl.name, "cells": wl.ncell, "storage": storage,
                        "surface": (f"{surf.num_vertices} vertices / {surf.num_elements} elements" if surf else None),
+                       "links_at_step0": link_stats,
                        "l2": "moment buffers exceed L2 (no flush needed)" if wl.ncell * bpc > 2 * 126e6
                        else "inputs smaller than L2", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",

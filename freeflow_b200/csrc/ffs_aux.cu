@@ -45,7 +45,10 @@ __global__ void prepare_flags_kernel(uint8_t *flags, uint32_t *wallmask, int nx,
         if (t == kFluid) {
             for (int r = 0; r < kNumOutletRules<DIM>; ++r) {
                 long long q = c + outlet_offset<DIM>(r, nx, nxy);
-                if (q >= 0 && q < n && (flags[q] & kTypeMask) == outlet_rule<DIM>(r).type) bits |= kBitOutletSrc;
+                if (q >= 0 && q < n && (flags[q] & kTypeMask) == outlet_rule<DIM>(r).type) {
+                    bits |= kBitOutletSrc;
+                    mask |= outlet_bit<DIM>(r);
+                }
             }
         }
         wallmask[c] = mask;

@@ -71,6 +71,51 @@ template <int DIM> __host__ __device__ constexpr int dir_index(int kx, int ky, i
     return t.v[kz][ky][kx];
 }
 
+// (c_x, c_y, c_z) of a direction index known only at run time (e.g. lane
+// = direction), decoded from 64-bit immediates: 6 bits per direction holding
+// c + 1 in base 4.  Unlike a __constant__ table this costs no memory access,
+// and lanes asking for different directions do not serialise.
+namespace dirpack {
+template <int DIM> struct Packed;
+template <> struct Packed<2> {
+    static constexpr unsigned long long word(int w)
+    {
+        unsigned long long r = 0;
+        for (int i = 0; i < 9; ++i)
+            r |= (unsigned long long)((Lattice<2>::cx(i) + 1) | ((Lattice<2>::cy(i) + 1) << 2) | (1 << 4)) << (6 * i);
+        return w == 0 ? r : 0ull;
+    }
+};
+template <> struct Packed<3> {
+    static constexpr unsigned long long word(int w)
+    {
+        unsigned long long r = 0;
+        for (int i = 10 * w; i < 10 * w + 10 && i < 27; ++i)
+            r |= (unsigned long long)((Lattice<3>::cx(i) + 1) | ((Lattice<3>::cy(i) + 1) << 2) | ((Lattice<3>::cz(i) + 1) << 4))
+                 << (6 * (i - 10 * w));
+        return r;
+    }
+};
+} // namespace dirpack
+
+template <int DIM> __host__ __device__ __forceinline__ void dir_vec(int i, int &cx, int &cy, int &cz)
+{
+    constexpr unsigned long long w0 = dirpack::Packed<DIM>::word(0);
+    constexpr unsigned long long w1 = dirpack::Packed<DIM>::word(1);
+    constexpr unsigned long long w2 = dirpack::Packed<DIM>::word(2);
+    unsigned long long w;
+    int sh;
+    if (DIM == 2) { w = w0; sh = 6 * i; }
+    else {
+        w = i < 10 ? w0 : (i < 20 ? w1 : w2);
+        sh = 6 * (i < 10 ? i : (i < 20 ? i - 10 : i - 20));
+    }
+    const unsigned v = (unsigned)(w >> sh) & 63u;
+    cx = (int)(v & 3u) - 1;
+    cy = (int)((v >> 2) & 3u) - 1;
+    cz = (int)(v >> 4) - 1;
+}
+
 // ------------------------------------------------------------------- flags
 enum Flag : uint8_t {
     kInvalid = 0, kFluid = 1, kFluidRest = 2, kSolid = 3, kSolidDynamic = 4, kWall = 5,
@@ -218,6 +263,27 @@ __device__ __forceinline__ void encode_store_strided(const float *m, T *base, si
 #pragma unroll
         for (int k = DIM + 1; k < NM; ++k)
             base[k * stride] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+    }
+}
+
+// The values encode_store writes, as they read back: m itself for FP32, the
+// decoded rounded deviations otherwise.
+template <int DIM, typename T>
+__device__ __forceinline__ void stored_values(const float *m, float *out, const Codec &c)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    if constexpr (!StorageTraits<T>::kEncoded) {
+#pragma unroll
+        for (int k = 0; k < NM; ++k) out[k] = m[k];
+    } else {
+        out[0] = 1.0f + StorageTraits<T>::from(StorageTraits<T>::to(m[0] - 1.0f));
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) out[1 + a] = StorageTraits<T>::from(StorageTraits<T>::to(m[1 + a] * c.su)) * c.inv_su;
+#pragma unroll
+        for (int k = DIM + 1; k < NM; ++k) {
+            const float ua = out[1 + MomentLayout<DIM>::pa(k)], ub = out[1 + MomentLayout<DIM>::pb(k)];
+            out[k] = fmaf(StorageTraits<T>::from(StorageTraits<T>::to((m[k] - ua * ub) * c.sp)), c.inv_sp, ua * ub);
+        }
     }
 }
 

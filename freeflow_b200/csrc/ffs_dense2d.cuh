@@ -59,9 +59,9 @@ __device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y
             float pop[9];
 #pragma unroll
             for (int i = 0; i < 9; ++i) pop[i] = sp[i][ty + 1 - L::cy(i)][tx + 1 - L::cx(i)];
+            const uint32_t wm = (f8 & (kBitNearWall | kBitOutletSrc)) ? g.wallmask[idx] : 0u;
             if (f8 & kBitNearWall) {
                 // bounce-back: f_i(x) = f_inv(i)^rec(x) when x - c_i is a wall
-                uint32_t wm = g.wallmask[idx];
 #pragma unroll
                 for (int i = 1; i < 9; ++i)
                     if (wm & (1u << i)) pop[i] = sp[L::inv(i)][ty + 1][tx + 1];
@@ -76,7 +76,11 @@ __device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y
             for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
             encode_store<2, T>(m, planes, idx, g.codec);
             if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
-            if (f8 & kBitOutletSrc) feed_outlets<2, T>(g, idx);
+            if (f8 & kBitOutletSrc) {
+                float ms[6];
+                stored_values<2, T>(m, ms, g.codec);
+                feed_outlets<2, T>(g, idx, ms, wm);
+            }
         }
     }
 }

@@ -8,44 +8,62 @@
 // then pulls them back out of shared memory.  Here a CTA owns a 32 x 8 column
 // of cells and marches up z through a chunk of planes:
 //
-//   * each plane is reconstructed once, for its 34 x 10 xy halo (1.33x the
-//     interior), by 170 threads that handle two halo cells each with packed
-//     FP32-pair arithmetic (add/fma.rn.f32x2), into one of two shared-memory
-//     buffers (2 x 27 x 340 floats = 72 KB, three CTAs per SM);
-//   * every population of plane p is consumed as soon as the plane exists:
-//     the c_z = -1 slice completes the raw moments of the cell below (plane
-//     p-1), the c_z = 0 slice feeds plane p, the c_z = +1 slice starts plane
-//     p+1.  Each thread keeps the partial raw moments of its column's next two
-//     cells in registers, so a plane is read once, one barrier per plane;
+//   * each plane is reconstructed once for its 34 x 10 xy halo: every thread
+//     reconstructs its own cell, and the first 84 threads one cell of the
+//     ring around the tile as well;
+//   * the populations of plane p go to one of two shared-memory buffers
+//     (2 x 27 x 340 floats) and are consumed as soon as they exist: the
+//     c_z = -1 slice completes the raw moments of the cell below (plane p-1),
+//     the c_z = 0 slice feeds plane p, the c_z = +1 slice starts plane p+1.
+//     Each thread keeps the partial raw moments of its column's next two
+//     cells in registers, so there is one barrier per plane;
+//   * bounce-back: a halo cell of a bounce-back type (wall, solid) gets zeros
+//     in its 27 population slots instead of a reconstruction, so whatever a
+//     fluid neighbour pulls from it adds nothing; each fluid cell next to a
+//     wall then adds its own reflected populations max(0, f_inv(i)^rec(x))
+//     once, while its own plane is in shared memory.  (A fluid cell on a
+//     non-periodic domain face whose wrapped neighbour is a wall pulls from
+//     its clamped, non-wall halo instead; that pulled value is removed
+//     explicitly.)  The result is the reference's f_i(x) = max(0,
+//     f_inv(i)^rec(x)) for wall neighbours x - c_i (FsiCoupling3D.cu:209-222);
 //   * moments are SoA planes in HBM (128 B coalesced per warp and moment);
-//     the next plane's moments and flag bytes are prefetched into registers
-//     while the current plane is processed;
-//   * wall neighbours are a per-cell bit mask, applied only to cells flagged
-//     near-wall (an exact correction of the pulled population by the
-//     bounce-back one), outlets are fed by their inner neighbour in the same
-//     pass, and cells with moving-boundary links are left to the sparse link
-//     kernel (ffs_links.cu).
+//     moments, flag bytes and wall masks are prefetched a plane ahead;
+//     outlets are fed by their inner neighbour in the same pass, and cells with
+//     moving-boundary links are left to the sparse link kernel (ffs_links.cu).
 #include "ffs_dense2d.cuh"
 #include "ffs_dense3d.cuh"
 
 namespace fflbm {
 
 namespace {
-constexpr int kTX = D3::kTX, kTY = D3::kTY, kHX = D3::kHX, kHalo = D3::kHalo, kHalf = D3::kHalf;
+constexpr int kTX = D3::kTX, kTY = D3::kTY, kHX = D3::kHX, kHalo = D3::kHalo, kRing = D3::kRing;
 constexpr int kPlane = D3::kPlaneFloats;
 
-// raw-moment slot of M_pqr: {rho, jx, jy, jz, Pxx, Pyy, Pzz, Pxy, Pyz, Pxz}
-// 9 populations of one c_z slice (f[ky][kx], clamped) -> the six x/y moments
+__device__ __forceinline__ int set_of(int kx, int ky, int kz) { return (kz * 3 + ky) * 3 + kx; }
+
+// halo index (hx, hy) of ring cell r: rows y0-1 and y0+8 (34 cells each),
+// then columns x0-1 and x0+32 (8 cells each)
+__device__ __forceinline__ int ring_cell(int r)
+{
+    if (r < 2 * kHX) return (r < kHX) ? r : (kHalo - kHX) + (r - kHX);
+    int q = r - 2 * kHX; // 0..15
+    int hy = 1 + (q & 7);
+    return hy * kHX + ((q < 8) ? 0 : kHX - 1);
+}
+
+// raw-moment slot: {rho, jx, jy, jz, Pxx, Pyy, Pzz, Pxy, Pyz, Pxz}
+// 9 populations of one c_z slice (clamped) -> x/y moments
 // Y = {Y00, Y01, Y02, Y10, Y11, Y20}
-__device__ __forceinline__ void slice_sums(const float *buf, int kz, int tx, int ty, float *Y)
+__device__ __forceinline__ void slice_sums(const float *buf, int kz, int c_own, float *Y)
 {
     float X0[3], X1[3], X2[3];
 #pragma unroll
     for (int ky = 0; ky < 3; ++ky) {
-        const float *row = buf + ((kz * 3 + ky) * 3) * kHalo + (ty + 2 - ky) * kHX + tx;
-        float fm = fmaxf(row[0 * kHalo + 2], 0.0f); // kx = 0 (c_x = -1): source x + 1
-        float f0 = fmaxf(row[1 * kHalo + 1], 0.0f); // kx = 1
-        float fp = fmaxf(row[2 * kHalo + 0], 0.0f); // kx = 2 (c_x = +1): source x - 1
+        // population (kx, ky, kz) of the cell at c_own - (kx-1) - (ky-1)*kHX
+        const int crow = c_own - (ky - 1) * kHX;
+        float fm = fmaxf(buf[set_of(0, ky, kz) * kHalo + crow + 1], 0.0f);
+        float f0 = fmaxf(buf[set_of(1, ky, kz) * kHalo + crow], 0.0f);
+        float fp = fmaxf(buf[set_of(2, ky, kz) * kHalo + crow - 1], 0.0f);
         float s = fp + fm;
         X1[ky] = fp - fm;
         X0[ky] = f0 + s;
@@ -60,7 +78,6 @@ __device__ __forceinline__ void slice_sums(const float *buf, int kz, int tx, int
     Y[5] = X2[1] + (X2[2] + X2[0]);
 }
 
-// add a slice with velocity component c_z to the raw moments R
 template <int CZ> __device__ __forceinline__ void slice_add(float *R, const float *Y)
 {
     R[0] += Y[0]; R[2] += Y[1]; R[5] += Y[2]; R[1] += Y[3]; R[7] += Y[4]; R[4] += Y[5];
@@ -68,53 +85,78 @@ template <int CZ> __device__ __forceinline__ void slice_add(float *R, const floa
         R[3] += CZ * Y[0]; R[6] += Y[0]; R[8] += CZ * Y[1]; R[9] += CZ * Y[3];
     }
 }
-// start R from a c_z = +1 slice
 __device__ __forceinline__ void slice_init_plus(float *R, const float *Y)
 {
     R[0] = Y[0]; R[2] = Y[1]; R[5] = Y[2]; R[1] = Y[3]; R[7] = Y[4]; R[4] = Y[5];
     R[3] = Y[0]; R[6] = Y[0]; R[8] = Y[1]; R[9] = Y[3];
 }
-} // namespace
 
-// Replace, in the raw moments R of near-wall cell (x, y, z), every population
-// pulled from a bounce-back neighbour by the reflected population of the cell
-// itself (FsiCoupling3D.cu:209-222): R += basis(c_i) (max(0, f_inv(i)^rec(x)) -
-// max(0, f_i^rec(x - c_i))), the second term being what the slice pass added.
-template <typename T>
-__device__ __noinline__ void wall_correct(const GridArgs<T> &g, float *R, int x, int y, int z, uint32_t idx)
+// R += s * basis(c) for the velocity (cx, cy, cz)
+__device__ __forceinline__ void add_basis(float *R, int cx, int cy, int cz, float s)
 {
-    const uint32_t wm = g.wallmask[idx];
-    const long long nxy = (long long)g.nx * g.ny;
-    const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
-    float m[10];
-    load_moments<3, T>(m, g.src, g.ncell, idx, g.codec);
-    Coef<3> own;
-    own.make(m);
+    R[0] += s;
+    R[1] += cx * s; R[2] += cy * s; R[3] += cz * s;
+    R[4] += cx * cx * s; R[5] += cy * cy * s; R[6] += cz * cz * s;
+    R[7] += cx * cy * s; R[8] += cy * cz * s; R[9] += cx * cz * s;
+}
+
+// Bounce-back corrections that the current plane (buf, plane p) allows:
+//   cell p-1 (Rp, mask wp): remove the pulled c_z = -1 populations of wall
+//                           directions (they came from plane p);
+//   cell p   (Rc, mask wc): remove the pulled c_z = 0 ones, add the cell's own
+//                           reflected populations f_inv(i)(x) (its plane is p);
+//   cell p+1 (Rn, mask wn): remove the pulled c_z = +1 ones.
+// Reference rule: FsiCoupling3D.cu:209-222, f_i(x) = max(0, f_inv(i)^rec(x)).
+// Only the set bits are visited (a wall face sets nine of them).
+__device__ __forceinline__ void add_basis_rt(float *R, int cx, int cy, int cz, float s)
+{
+    const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
+    R[0] += s;
+    R[1] = fmaf(fx, s, R[1]); R[2] = fmaf(fy, s, R[2]); R[3] = fmaf(fz, s, R[3]);
+    R[4] = fmaf(fx * fx, s, R[4]); R[5] = fmaf(fy * fy, s, R[5]); R[6] = fmaf(fz * fz, s, R[6]);
+    R[7] = fmaf(fx * fy, s, R[7]); R[8] = fmaf(fy * fz, s, R[8]); R[9] = fmaf(fx * fz, s, R[9]);
+}
+
+// R += basis(c_i) max(0, f_inv(i)^rec(x)) for every wall direction i in w,
+// with the cell's own populations read from the current plane.
+__device__ __forceinline__ void add_reflected(const float *buf, int c_own, uint32_t w, float (&R)[10])
+{
 #pragma unroll
     for (int kz = 0; kz < 3; ++kz)
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky)
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
-                if (!(wm & (1u << dir_index<3>(kx, ky, kz)))) continue;
-                const int cx = kx - 1, cy = ky - 1, cz = kz - 1;
-                const int sx = halo_index(x - cx, g.nx, wx), sy = halo_index(y - cy, g.ny, wy);
-                const int sz = halo_index(z - cz, g.nz, wz);
-                float mn[10];
-                load_moments<3, T>(mn, g.src, g.ncell, (uint32_t)(sz * nxy + (long long)sy * g.nx + sx), g.codec);
-                Coef<3> nb;
-                nb.make(mn);
-                const float d = fmaxf(own.population(-cx, -cy, -cz), 0.0f) - fmaxf(nb.population(cx, cy, cz), 0.0f);
-                R[0] += d;
-                R[1] += cx * d; R[2] += cy * d; R[3] += cz * d;
-                R[4] += cx * cx * d; R[5] += cy * cy * d; R[6] += cz * cz * d;
-                R[7] += cx * cy * d; R[8] += cy * cz * d; R[9] += cx * cz * d;
+                const int i = dir_index<3>(kx, ky, kz);
+                if (i == 0) continue;
+                float f = fmaxf(buf[set_of(2 - kx, 2 - ky, 2 - kz) * kHalo + c_own], 0.0f);
+                f = (w & (1u << i)) ? f : 0.0f;
+                add_basis(R, kx - 1, ky - 1, kz - 1, f);
             }
 }
 
-// MINB = CTAs per SM the register budget is cut for: 3 (80 registers, a few
-// spills) or 2 (no spills); launch_dense3d times both on the grid and keeps
-// the faster (tune_dense3d).
+__device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint32_t w, int kz_sel, bool own, float (&R)[10],
+                                           float (&Rc)[10])
+{
+    while (w) {
+        const int i = __ffs(w) - 1;
+        w &= w - 1;
+        int cx, cy, cz;
+        dir_vec<3>(i, cx, cy, cz);
+        if (kz_sel >= 0 && cz + 1 == kz_sel) {
+            const float pulled = fmaxf(buf[set_of(cx + 1, cy + 1, cz + 1) * kHalo + c_own - cx - cy * kHX], 0.0f);
+            add_basis_rt(R, cx, cy, cz, -pulled);
+        }
+        if (own) {
+            const float f = fmaxf(buf[set_of(1 - cx, 1 - cy, 1 - cz) * kHalo + c_own], 0.0f);
+            add_basis_rt(Rc, cx, cy, cz, f);
+        }
+    }
+}
+} // namespace
+
+// MINB = CTAs per SM the register budget is cut for; launch_dense3d times the
+// variants on the grid and keeps the faster (tune_dense3d).
 template <typename T, int MINB>
 __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T> g, int zchunk)
 {
@@ -126,94 +168,157 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     const long long nxy = (long long)g.nx * g.ny;
     const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
 
-    // reconstruction role: threads 0..169 own halo cells tid and tid + 170
-    const bool rec = tid < kHalf;
+    const int tx = tid % kTX, ty = tid / kTX;
+    const int x = x0 + tx, y = y0 + ty;
+    const bool inside = x < g.nx && y < g.ny;
+    const int c_own = (ty + 1) * kHX + (tx + 1);
+    // partner cell of the reconstruction pair
+    const bool has_ring = tid < kRing;
+    const int c_ring = has_ring ? ring_cell(tid) : c_own;
     auto planar = [&](int c) {
         int hx = c % kHX, hy = c / kHX;
         return (uint32_t)(halo_index(y0 + hy - 1, g.ny, wy) * g.nx + halo_index(x0 + hx - 1, g.nx, wx));
     };
-    const uint32_t off0 = rec ? planar(tid) : 0u, off1 = rec ? planar(tid + kHalf) : 0u;
+    const uint32_t off_own = planar(c_own), off_ring = planar(c_ring);
+    const uint32_t col = inside ? (uint32_t)(y * g.nx + x) : 0u;
+    // directions whose pull leaves the grid in x or y on a non-periodic axis
+    // (the halo is clamped there, so the pulled population is the cell's own)
+    uint32_t oor_xy = 0;
+    if (inside && ((!wx && (x == 0 || x == g.nx - 1)) || (!wy && (y == 0 || y == g.ny - 1)))) {
+#pragma unroll
+        for (int i = 1; i < 27; ++i) {
+            int cx, cy, cz;
+            dir_vec<3>(i, cx, cy, cz);
+            if ((!wx && (x - cx < 0 || x - cx >= g.nx)) || (!wy && (y - cy < 0 || y - cy >= g.ny))) oor_xy |= 1u << i;
+        }
+    }
+    uint32_t oor_zlo = 0, oor_zhi = 0; // directions pulling from below z = 0 / above z = nz-1
+    if (!wz) {
+#pragma unroll
+        for (int i = 1; i < 27; ++i) {
+            int cx, cy, cz;
+            dir_vec<3>(i, cx, cy, cz);
+            if (cz == 1) oor_zlo |= 1u << i;
+            if (cz == -1) oor_zhi |= 1u << i;
+        }
+    }
+
     float mA[10], mB[10];
+    uint32_t hA = 0, hB = 0; // node types of the two halo cells (bounce-back cells get zero slots)
     auto load_plane = [&](int z) {
-        if (!rec) return;
-        const T *base = g.src + (size_t)halo_index(z, g.nz, wz) * nxy;
+        const size_t zo = (size_t)halo_index(z, g.nz, wz) * nxy;
+        const T *base = g.src + zo;
 #pragma unroll
         for (int k = 0; k < 10; ++k) {
-            mA[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off0]);
-            mB[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off1]);
+            mA[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off_own]);
+            if (has_ring) mB[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off_ring]);
         }
+        hA = g.flags[zo + off_own] & kTypeMask;
+        if (has_ring) hB = g.flags[zo + off_ring] & kTypeMask;
+    };
+    auto recon_cell = [&](float *buf, float *m, uint32_t type, int c) {
+        if (is_bounce_back<3>(type)) {
+#pragma unroll
+            for (int j = 0; j < 27; ++j) buf[j * kHalo + c] = 0.0f;
+            return;
+        }
+        decode_moments<3, T>(m, g.codec);
+        Coef3V<float> cf;
+        cf.make(m);
+        cf.populations_each([&](int kz, int ky, int kx, float v) { buf[set_of(kx, ky, kz) * kHalo + c] = v; });
     };
     auto recon_plane = [&](float *buf) {
-        if (!rec) return;
-        decode_moments<3, T>(mA, g.codec);
-        decode_moments<3, T>(mB, g.codec);
-        f2 m[10];
-#pragma unroll
-        for (int k = 0; k < 10; ++k) m[k] = f2make(mA[k], mB[k]);
-        Coef3V<f2> cf;
-        cf.make(m);
-        cf.populations_each([&](int kz, int ky, int kx, f2 v) {
-            float a, b;
-            f2split(v, a, b);
-            float *set = buf + ((kz * 3 + ky) * 3 + kx) * kHalo;
-            set[tid] = a;
-            set[tid + kHalf] = b;
-        });
+        recon_cell(buf, mA, hA, c_own);
+        if (has_ring) recon_cell(buf, mB, hB, c_ring);
+    };
+    auto flag_at = [&](int z) -> uint32_t {
+        return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[(size_t)z * nxy + col] : 0u;
     };
 
-    const int tx = tid % kTX, ty = tid / kTX;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool inside = x < g.nx && y < g.ny;
-    const uint32_t col = inside ? (uint32_t)(y * g.nx + x) : 0u;
-
-    float Ap[10], Ac[10];  // partial raw moments of the cells at z = p-1 and z = p
-    uint8_t fp = 0, fc = 0; // their flag bytes
+    // Two register sets hold the partial raw moments of the column's cells at
+    // z = p-1 and z = p; their roles swap every plane (loop unrolled by two).
+    float X[10], Y[10];
 #pragma unroll
-    for (int k = 0; k < 10; ++k) Ap[k] = Ac[k] = 0.0f;
+    for (int k = 0; k < 10; ++k) X[k] = Y[k] = 0.0f;
+    // flag bytes of z = p-1, p, p+1 and wall masks of z = p-1, p
+    uint32_t fp = 0, fc = 0, fn = flag_at(zb);
+    uint32_t wp = 0, wc = 0;
 
-    load_plane(zb - 1);
-    for (int p = zb - 1; p <= ze; ++p) {
+    // one plane: Rp = sums of z = p-1 (completed here), Rc = sums of z = p,
+    // Rn receives the new c_z = +1 slice (the cell at z = p+1)
+    auto plane = [&](int p, float (&Rp)[10], float (&Rc)[10]) {
         float *buf = smem + (p & 1) * kPlane;
         recon_plane(buf);
         if (p < ze) load_plane(p + 1);
-        uint8_t fn = 0;
-        if (inside && p + 1 < ze) fn = g.flags[(size_t)(p + 1) * nxy + col];
+        const uint32_t fnn = flag_at(p + 2);
+        // mask word (wall and outlet bits) of the cell at z = p+1; only cells
+        // this pass updates use it (walls, inlets and outlets carry mask bits
+        // of their own neighbours that must not trigger any work)
+        const bool upd_n = is_updated(fn & kTypeMask) && !(fn & kBitLink);
+        const uint32_t wn = (upd_n && (fn & (kBitNearWall | kBitOutletSrc))) ? g.wallmask[(size_t)(p + 1) * nxy + col] : 0u;
         __syncthreads();
         if (inside) {
-            float Y[6];
-            // c_z = -1 slice completes the cell at z = p - 1
-            slice_sums(buf, 0, tx, ty, Y);
-            slice_add<-1>(Ap, Y);
+            // wall directions whose pull would leave the grid on a non-periodic
+            // axis, per destination cell: z = p-1 (c_z = -1 slice), z = p
+            // (c_z = 0), z = p+1 (c_z = +1)
+            const uint32_t oor_p = oor_xy | ((p - 1 == g.nz - 1) ? oor_zhi : 0u);
+            const uint32_t oor_c = oor_xy;
+            const uint32_t oor_n = oor_xy | ((p + 1 == 0) ? oor_zlo : 0u);
+            float S[6];
+            slice_sums(buf, 0, c_own, S);
+            slice_add<-1>(Rp, S);
+            slice_sums(buf, 1, c_own, S);
+            slice_add<0>(Rc, S);
+            constexpr uint32_t kWall = wall_bits_mask<3>();
+            if (wc & kWall) add_reflected(buf, c_own, wc & kWall, Rc);
+            // wall directions whose clamped halo source is the cell itself:
+            // remove the pulled (non-zero) value
+            if (wp & kWall & oor_p) wall_fix_part(buf, c_own, wp & kWall & oor_p, 0, false, Rp, Rc);
+            if (wc & kWall & oor_c) wall_fix_part(buf, c_own, wc & kWall & oor_c, 1, false, Rc, Rc);
+            // the cell at z = p - 1 is complete
             const int d = p - 1;
             if (d >= zb && is_updated(fp & kTypeMask) && !(fp & kBitLink)) {
                 const uint32_t idx = (uint32_t)(d * nxy + col);
-                if (fp & kBitNearWall) wall_correct<T>(g, Ap, x, y, d, idx);
                 float m[10];
-                collide3(Ap, g.omega, m);
+                collide3(Rp, g.omega, m);
                 encode_store_strided<3, T>(m, g.dst + idx, g.ncell, g.codec);
                 if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
-                if (fp & kBitOutletSrc) feed_outlets<3, T>(g, idx);
+                if (fp & kBitOutletSrc) {
+                    float ms[10];
+                    stored_values<3, T>(m, ms, g.codec);
+                    feed_outlets<3, T>(g, idx, ms, wp);
+                }
             }
-            // c_z = 0 slice feeds z = p; c_z = +1 slice starts z = p + 1
-            slice_sums(buf, 1, tx, ty, Y);
-            slice_add<0>(Ac, Y);
-#pragma unroll
-            for (int k = 0; k < 10; ++k) Ap[k] = Ac[k];
-            slice_sums(buf, 2, tx, ty, Y);
-            slice_init_plus(Ac, Y);
-            fp = fc;
-            fc = fn;
+            // Rp is free: it becomes the cell at z = p + 1
+            slice_sums(buf, 2, c_own, S);
+            slice_init_plus(Rp, S);
+            if (wn & kWall & oor_n) wall_fix_part(buf, c_own, wn & kWall & oor_n, 2, false, Rp, Rp);
         }
+        fp = fc; fc = fn; fn = fnn;
+        wp = wc; wc = wn;
+    };
+
+    load_plane(zb - 1);
+    int p = zb - 1;
+    for (; p + 1 <= ze; p += 2) {
+        plane(p, X, Y);     // completes X (z = p-1); X := z = p+1
+        plane(p + 1, Y, X); // completes Y (z = p);   Y := z = p+2
     }
+    if (p <= ze) plane(p, X, Y);
 }
 
 // Number of z chunks that best fills the GPU: whole waves of CTAs, with the
 // two extra planes each chunk reconstructs counted as overhead.
 static int choose_zchunks(int tiles, int nz, int slots)
 {
-    int best = 1;
+    // CTAs next to walls and outlets carry extra work; several waves of CTAs
+    // let the scheduler even that out, so aim for three waves or more while
+    // chunks keep at least 16 planes
+    int nmin = 1;
+    while ((long long)tiles * nmin < 3LL * slots && nz / (nmin + 1) >= 16) ++nmin;
+    int best = nmin;
     double best_eff = 0.0;
-    for (int n = 1; n <= 16 && n <= nz; ++n) {
+    for (int n = nmin; n <= nmin + 8 && n <= nz; ++n) {
         int chunk = (nz + n - 1) / n;
         long long ctas = (long long)tiles * ((nz + chunk - 1) / chunk);
         long long waves = (ctas + slots - 1) / slots;
@@ -265,7 +370,7 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     float best = 1e30f;
     int best_v = 0;
     for (int v = 0; v < 2; ++v) {
-        if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue;  // warm-up
+        if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue; // warm-up
         cudaEventRecord(a, s);
         for (int r = 0; r < 3; ++r) launch_dense3d<T>(g, s, v);
         cudaEventRecord(b, s);

@@ -7,11 +7,11 @@ namespace fflbm {
 struct D3 {
     static constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
     static constexpr int kHX = kTX + 2, kHY = kTY + 2, kHalo = kHX * kHY;
-    static constexpr int kHalf = kHalo / 2;                   // halo cells per reconstructing thread pair
+    static constexpr int kRing = kHalo - kTX * kTY;           // halo cells outside the tile (84)
     static constexpr int kPlaneFloats = 27 * kHalo;           // all populations of one halo plane
     static constexpr size_t kSmemBytes = 2 * (size_t)kPlaneFloats * sizeof(float); // double buffer
 };
-static_assert(D3::kHalo % 2 == 0, "halo plane must split into pairs");
+static_assert(D3::kRing <= D3::kThreads, "every ring cell needs a partner thread");
 
 // variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM
 template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant);

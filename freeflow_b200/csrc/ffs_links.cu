@@ -37,20 +37,6 @@
 
 namespace fflbm {
 
-__constant__ signed char kDir2[9][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {-1, 0, 0}, {0, -1, 0},
-                                         {1, 1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, -1, 0}};
-__constant__ signed char kDir3[27][3] = {
-    {0, 0, 0},   {1, 0, 0},   {-1, 0, 0},  {0, 1, 0},   {0, -1, 0},  {0, 0, 1},   {0, 0, -1},
-    {1, 1, 0},   {-1, -1, 0}, {1, 0, 1},   {-1, 0, -1}, {0, 1, 1},   {0, -1, -1}, {1, -1, 0},
-    {-1, 1, 0},  {1, 0, -1},  {-1, 0, 1},  {0, 1, -1},  {0, -1, 1},  {1, 1, 1},   {-1, -1, -1},
-    {1, 1, -1},  {-1, -1, 1}, {1, -1, 1},  {-1, 1, -1}, {-1, 1, 1},  {1, -1, -1}};
-
-template <int DIM> __device__ __forceinline__ void dir_vec(int i, int &cx, int &cy, int &cz)
-{
-    if (DIM == 2) { cx = kDir2[i][0]; cy = kDir2[i][1]; cz = 0; }
-    else { cx = kDir3[i][0]; cy = kDir3[i][1]; cz = kDir3[i][2]; }
-}
-
 __device__ __forceinline__ uint32_t hash_cell(uint32_t c)
 {
     c ^= c >> 16; c *= 0x7feb352dU; c ^= c >> 15; c *= 0x846ca68bU; c ^= c >> 16;
@@ -127,6 +113,7 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
             continue;
         }
         const geom::TriPre tr = geom::tri_pre(s.V, ia, ib, ic);
+        const float inv_den = __fdividef(1.0f, tr.den);
         float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
         float bmax[3] = {1.175494351e-38f, 1.175494351e-38f, 1.175494351e-38f};
         const uint32_t vid[3] = {ia, ib, ic};
@@ -156,15 +143,26 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
             const int k3 = lo[2] + c / (ext[0] * ext[1]);
             int cx, cy, cz;
             dir_vec<3>(l, cx, cy, cz);
-            // prefilter (ordinary float math; only ever rejects clear misses)
-            const float s1 = tr.n[0] * ((float)i * cl - tr.v0[0]) + tr.n[1] * ((float)j * cl - tr.v0[1]) +
-                             tr.n[2] * ((float)k3 * cl - tr.v0[2]);
+            // prefilter in ordinary (fast) float math; it only rejects clear
+            // misses: the plane is not reached (t outside [0, 1] by more than a
+            // margin of 2e-3 cells) or the plane point lies outside the
+            // triangle by more than 1% in barycentric terms
+            const float px = (float)i * cl - tr.v0[0], py = (float)j * cl - tr.v0[1], pz = (float)k3 * cl - tr.v0[2];
+            const float s1 = tr.n[0] * px + tr.n[1] * py + tr.n[2] * pz;
             const float a = cl * (tr.n[0] * cx + tr.n[1] * cy + tr.n[2] * cz);
-            // exact t = s1 / a (approximately); a miss needs t < 0 or t > 1
-            if (fabsf(a) > margin) {
-                const float t = s1 / a;
-                const float tol = margin / fabsf(a);
+            const float fa = fabsf(a);
+            if (fa > margin) {
+                const float t = __fdividef(s1, a);
+                const float tol = __fdividef(margin, fa);
                 if (t < -tol || t > 1.0f + tol) continue;
+                // plane point relative to v0: p1 - t c cl - v0
+                const float tc = t * cl;
+                const float wx = px - tc * cx, wy = py - tc * cy, wz = pz - tc * cz;
+                const float d20 = wx * tr.e1[0] + wy * tr.e1[1] + wz * tr.e1[2];
+                const float d21 = wx * tr.e2[0] + wy * tr.e2[1] + wz * tr.e2[2];
+                const float u = (tr.d11 * d20 - tr.d01 * d21) * inv_den;
+                const float v = (tr.d00 * d21 - tr.d01 * d20) * inv_den;
+                if (u < -0.01f || v < -0.01f || u + v > 1.01f) continue;
             } else if (fabsf(s1) > 2.0f * margin) {
                 continue; // link parallel to the plane and away from it
             }
@@ -236,61 +234,41 @@ __global__ void detect_links_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTab
 }
 
 // -------------------------------------------------------------- link cells
+// Per-vertex force shares of the links of one cell.  Lanes whose links hit
+// the same element (found with __match_any_sync) are summed with the warp's
+// integer reduction unit (__reduce_add_sync), one value per (vertex slot,
+// component), in 2^-24 fixed point; the group leader then adds each sum, in
+// 2^-32 fixed point, to the vertex accumulator with one 64-bit integer
+// atomic.  Integer sums are associative, so the per-vertex result does not
+// depend on warp, lane or launch order.  A share beyond +-127 lattice units
+// (outside the 2^-24 range of 27 summed int32 shares) is clamped and flagged.
 template <int DIM>
-__device__ __forceinline__ void add_force_share(long long *acc, uint32_t vert, int k, float share, uint32_t *status)
-{
-    // |share| < 2^30 lattice units keeps the 2^-32 fixed point inside int64
-    float v = share;
-    if (!(fabsf(v) < 1073741824.0f)) {
-        atomicOr(status, kStatusForceRange);
-        v = isfinite(v) ? copysignf(1073741824.0f, v) : 0.0f;
-    }
-    long long q = __double2ll_rn((double)v * kForceScale);
-    atomicAdd(reinterpret_cast<unsigned long long *>(acc + (size_t)vert * DIM + k), (unsigned long long)q);
-}
-
-// warp-aggregated version: lanes that hit the same vertex combine first
-template <int DIM>
-__device__ __forceinline__ void add_force_share_warp(long long *acc, bool active, uint32_t vert, const float *share,
-                                                     uint32_t *status)
+__device__ __forceinline__ void add_forces_warp(long long *acc, bool active, uint32_t elem, const uint32_t *vert,
+                                                const float (*share)[3], uint32_t *status)
 {
     const unsigned full = 0xffffffffu;
-    long long q[DIM];
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        float v = active ? share[k] : 0.0f;
-        if (!(fabsf(v) < 1073741824.0f)) {
-            atomicOr(status, kStatusForceRange);
-            v = isfinite(v) ? copysignf(1073741824.0f, v) : 0.0f;
-        }
-        q[k] = __double2ll_rn((double)v * kForceScale);
-    }
-    const uint32_t key = active ? vert : 0xffffffffu;
-    const unsigned peers = __match_any_sync(full, key);
+    const unsigned peers = __match_any_sync(full, active ? elem : 0xffffffffu);
     const int lane = threadIdx.x & 31;
-    const int leader = __ffs(peers) - 1;
-    // sum over the peer group: each peer adds its value to the leader by shuffle
-    // loop over the group in lane order (deterministic integer sums anyway)
+    const bool leader = active && lane == __ffs(peers) - 1;
 #pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        long long sum = 0;
-        unsigned m = peers;
-        while (m) {
-            int src = __ffs(m) - 1;
-            m &= m - 1;
-            sum += __shfl_sync(peers, q[k], src);
+    for (int j = 0; j < DIM; ++j)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            float v = active ? share[j][k] : 0.0f;
+            if (!(fabsf(v) < 127.0f)) {
+                if (active) atomicOr(status, kStatusForceRange);
+                v = isfinite(v) ? copysignf(127.0f, v) : 0.0f;
+            }
+            const int q = __float2int_rn(v * 16777216.0f); // 2^24
+            const int sum = (int)__reduce_add_sync(peers, (unsigned)q);
+            if (leader && sum != 0)
+                atomicAdd(reinterpret_cast<unsigned long long *>(acc + (size_t)vert[j] * DIM + k),
+                          (unsigned long long)((long long)sum * 256)); // 2^24 -> 2^32
         }
-        q[k] = sum;
-    }
-    if (active && lane == leader) {
-#pragma unroll
-        for (int k = 0; k < DIM; ++k)
-            if (q[k] != 0) atomicAdd(reinterpret_cast<unsigned long long *>(acc + (size_t)vert * DIM + k), (unsigned long long)q[k]);
-    }
 }
 
 template <int DIM, typename T, bool HALF>
-__global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
+__global__ void __launch_bounds__(256, 3) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
                                                          StepScalars sc)
 {
     constexpr int Q = Lattice<DIM>::Q, NM = Lattice<DIM>::NM;
@@ -314,6 +292,7 @@ __global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t
             own.make(mc);
             float pop = 0.0f;
             bool has_share = false;
+            uint32_t hit_elem = 0xffffffffu;
             uint32_t vshare[3] = {0, 0, 0};
             float share[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; // [vertex][component]
             if (lane < Q) {
@@ -379,6 +358,7 @@ __global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t
 #pragma unroll
                             for (int k = 0; k < DIM; ++k) F[k] = fin * (-c3[k] - uw[k]) - fout * (c3[k] - uw[k]);
                             has_share = true;
+                            hit_elem = e;
 #pragma unroll
                             for (int j = 0; j < DIM; ++j) {
                                 vshare[j] = vv[j];
@@ -401,9 +381,8 @@ __global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t
                     pop = fmaxf(v, 0.0f);
                 }
             }
-            // forces: one share per (link, element vertex)
-#pragma unroll
-            for (int j = 0; j < DIM; ++j) add_force_share_warp<DIM>(lt.acc, has_share, vshare[j], share[j], g.status);
+            // forces: one share per (link, element vertex), summed per element
+            add_forces_warp<DIM>(lt.acc, has_share, hit_elem, vshare, share, g.status);
             // raw moments by warp reduction
             int cx = 0, cy = 0, cz = 0;
             if (lane < Q) dir_vec<DIM>(lane, cx, cy, cz);
@@ -430,7 +409,11 @@ __global__ void __launch_bounds__(256) link_cells_kernel(GridArgs<T> g, uint32_t
                 for (int k = 0; k < NM; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
                 encode_store<DIM, T>(m, planes, cell, g.codec);
                 if (bad_state<DIM>(m)) atomicOr(g.status, kStatusNonFinite);
-                if (f8 & kBitOutletSrc) feed_outlets<DIM, T>(g, cell);
+                if (f8 & kBitOutletSrc) {
+                    float ms[NM];
+                    stored_values<DIM, T>(m, ms, g.codec);
+                    feed_outlets<DIM, T>(g, cell, ms, g.wallmask[cell]);
+                }
             }
         }
         // return the slot to the empty state and drop the cell's LINK bit

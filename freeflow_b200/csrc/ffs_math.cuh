@@ -324,10 +324,18 @@ __device__ __forceinline__ void raw_moments3(const float (*F)[3][3], float *R)
 // LbmFlowField3D.cpp:85-86).  Written in the algebraically equal form
 // pi' = (dev * (1 - omega) / rho) + equilibrium part, which avoids
 // subtracting c_s^2 from a value near c_s^2.
+// 1 / rho from the hardware approximation refined by one Newton step (within
+// an ulp of the IEEE quotient, without the division's slow-path branch)
+__device__ __forceinline__ float recip(float x)
+{
+    float r = __fdividef(1.0f, x);
+    return r * fmaf(-x, r, 2.0f);
+}
+
 __device__ __forceinline__ void collide2(const float *R, float omega, float *m)
 {
     float rho = R[0];
-    float ir = 1.0f / rho;
+    float ir = recip(rho);
     float ux = R[1] * ir, uy = R[2] * ir;
     float omw = 1.0f - omega;
     float ux2 = ux * ux, uy2 = uy * uy;
@@ -344,7 +352,7 @@ __device__ __forceinline__ void collide3(const float *R, float omega, float *m)
 {
     const float third = 1.0f / 3.0f;
     float rho = R[0];
-    float ir = 1.0f / rho;
+    float ir = recip(rho);
     float ux = R[1] * ir, uy = R[2] * ir, uz = R[3] * ir;
     float omw = 1.0f - omega;
     float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;

@@ -66,39 +66,54 @@ template <int DIM> __device__ __forceinline__ OutletRule outlet_rule(int r)
 
 template <int DIM> constexpr int kNumOutletRules = DIM == 2 ? 4 : 6;
 
-// Called by the thread that just stored cell p's new moments into g.dst.
-// All moment indices are resolved with unrolled compares so that nothing is
-// indexed dynamically (which would push arrays to local memory).
+// Outlet rules a cell feeds, kept in the spare bits of its wall-mask word
+// (bit i < Q of that word is the bounce-back mask of direction i; bit 0 is
+// never a wall because direction 0 does not move):
+//   D2Q9 : rules 0..3 at bits 16..19;  D3Q27: rules 0..4 at bits 27..31, rule 5 at bit 0.
+template <int DIM> __host__ __device__ constexpr uint32_t outlet_bit(int r)
+{
+    return DIM == 2 ? (1u << (16 + r)) : (r < 5 ? (1u << (27 + r)) : 1u);
+}
+template <int DIM> __host__ __device__ constexpr uint32_t outlet_bits_mask()
+{
+    return DIM == 2 ? 0xF0000u : 0xF8000001u;
+}
+template <int DIM> __host__ __device__ constexpr uint32_t wall_bits_mask()
+{
+    return DIM == 2 ? 0x1FEu : 0x07FFFFFEu;
+}
+
+// Called by the thread that has just stored cell p's new moments into g.dst.
+// `ms` are the stored values as they read back (after storage rounding) and
+// `word` the cell's mask word, whose outlet bits name the outlet neighbours
+// q = p + offset(rule) to update.  No flag or moment of p is re-read.
 template <int DIM, typename T>
-__device__ __forceinline__ void feed_outlets(const GridArgs<T> &g, uint32_t p)
+__device__ __forceinline__ void feed_outlets(const GridArgs<T> &g, uint32_t p, const float *ms, uint32_t word)
 {
     constexpr int NM = Lattice<DIM>::NM;
     const long long nxy = (long long)g.nx * g.ny;
-#pragma unroll 1
+#pragma unroll
     for (int r = 0; r < kNumOutletRules<DIM>; ++r) {
-        long long q = (long long)p + outlet_offset<DIM>(r, g.nx, nxy);
-        if (q < 0 || q >= (long long)g.ncell) continue;
+        if (!(word & outlet_bit<DIM>(r))) continue;
+        const uint32_t q = (uint32_t)((long long)p + outlet_offset<DIM>(r, g.nx, nxy));
         const OutletRule rule = outlet_rule<DIM>(r);
-        if ((g.flags[q] & kTypeMask) != rule.type) continue;
-        // the stored (rounded) normal velocity of p
-        float up = StorageTraits<T>::from(g.dst[(size_t)rule.comp * g.ncell + p]);
-        if constexpr (StorageTraits<T>::kEncoded) up *= g.codec.inv_su;
+        float up = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NM; ++k)
+            if (k == rule.comp) up = ms[k];
         const bool outward = (rule.sign > 0 && up > 0.0f) || (rule.sign < 0 && up < 0.0f);
         if constexpr (!StorageTraits<T>::kEncoded) {
             if (outward) g.dst[(size_t)rule.comp * g.ncell + q] = up;
             g.dst[(size_t)rule.pcomp * g.ncell + q] = up * up;
         } else {
             float mq[NM];
-            load_moments<DIM, T>(mq, g.dst, g.ncell, (uint32_t)q, g.codec);
+            load_moments<DIM, T>(mq, g.dst, g.ncell, q, g.codec);
 #pragma unroll
             for (int k = 0; k < NM; ++k) {
                 if (k == rule.comp && outward) mq[k] = up;
                 if (k == rule.pcomp) mq[k] = up * up;
             }
-            T *planes[NM];
-#pragma unroll
-            for (int k = 0; k < NM; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
-            encode_store<DIM, T>(mq, planes, (uint32_t)q, g.codec);
+            encode_store_strided<DIM, T>(mq, g.dst + q, g.ncell, g.codec);
         }
     }
 }
