@@ -70,23 +70,63 @@ def hbm_peak():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """SM clock and clock-event (throttle) samples while the timed region runs.
 
+    Polls NVML every 2 ms from a thread (reads only; no setting is changed), so
+    that timed regions of a fraction of a second still get tens of samples;
+    falls back to ``nvidia-smi -lms 100`` when NVML is not importable."""
+
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.sm, self.mask = [], 0
+        self.smax = None
         self.proc = None
         self.lines = []
+        self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _poll(self, nv, h):
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                self.mask |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                pass
+            self._stop.wait(0.002)
 
     def start(self):
         try:
+            nv, h = self._handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._nvml = nv
+            self._t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self._t.start()
+            return
+        except Exception:
+            self._nvml = None
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", "-i", str(self.cuda_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except Exception:
@@ -97,8 +137,14 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self._nvml is not None:
+            self._stop.set()
+            self._t.join(timeout=2)
+            reasons = sorted(n for n, bit in self.REASONS if self.mask & bit)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(self.sm), "source": "nvml 2 ms"}
         if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -121,7 +167,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi 100 ms"}
 
 
 # ------------------------------------------------------------ CPU (oracle)

@@ -111,7 +111,7 @@ def cylinder_channel_2d(nx=256, ny=128, radius=16.0, center=(64.0, 64.0), u_in=0
     u[fl] += rng.uniform(-perturbation, perturbation, size=(int(fl.sum()), 2))
     m = equilibrium_moments(np.ones(flags.size), u)
     v, e = circle_polygon(center[0] * fluid_dx, center[1] * fluid_dx, radius * fluid_dx, nseg)
-    return Workload("A:D2Q9 256x128 cylinder", 2, nx, ny, 1, nu, density, fluid_dx, dt, [u_in, 0, 0, 0],
+    return Workload(f"A:D2Q9 {nx}x{ny} cylinder", 2, nx, ny, 1, nu, density, fluid_dx, dt, [u_in, 0, 0, 0],
                     flags, m, 0, e, v, None, dict(seed=seed, reynolds=reynolds))
 
 
@@ -164,7 +164,7 @@ def swimmer_2d(nx=1200, ny=400, body_frac=0.4, n_boundary=198, freq=1.0, seed=0,
         return pos.astype(np.float32), vel.astype(np.float32)
 
     m = equilibrium_moments(np.ones(flags.size), np.zeros((flags.size, 2)))
-    return Workload("B:D2Q9 1200x400 swimmer", 2, nx, ny, 1, viscosity, density, fluid_dx, dt, [0, 0, 0, 0],
+    return Workload(f"B:D2Q9 {nx}x{ny} swimmer", 2, nx, ny, 1, viscosity, density, fluid_dx, dt, [0, 0, 0, 0],
                     flags, m, 0, e, rest.astype(np.float32), kin, dict(seed=seed, body_length_cells=L))
 
 
@@ -181,7 +181,7 @@ def taylor_green_3d(n=128, u0=0.04, viscosity=0.005, rho0=1.0):
     u = np.stack([ux, uy, uz], axis=-1).reshape(-1, 3)
     m = equilibrium_moments(rho.reshape(-1), u)
     flags = np.full(n ** 3, FLUID, dtype=np.uint8)
-    return Workload("C:D3Q27 128^3 Taylor-Green", 3, n, n, n, viscosity, 1.0, 1.0, 1.0, [0] * 6, flags, m, 7,
+    return Workload(f"C:D3Q27 {n}^3 Taylor-Green", 3, n, n, n, viscosity, 1.0, 1.0, 1.0, [0] * 6, flags, m, 7,
                     None, None, None, dict(u0=u0, k=2 * np.pi / n))
 
 
@@ -253,7 +253,7 @@ def swimmer_3d(nx=384, ny=192, nz=192, body_frac=0.3, freq=1.0, seed=0, fluid_dx
     u = np.zeros((flags.size, 3))
     u[flags == INLET_LEFT, 0] = u_in
     m = equilibrium_moments(np.ones(flags.size), u)
-    return Workload("D:D3Q27 384x192x192 swimmer", 3, nx, ny, nz, viscosity, density, fluid_dx, dt,
+    return Workload(f"D:D3Q27 {nx}x{ny}x{nz} swimmer", 3, nx, ny, nz, viscosity, density, fluid_dx, dt,
                     [u_in, 0, 0, 0, 0, 0], flags, m, 0, e, rest.astype(np.float32), kin,
                     dict(seed=seed, body_length_cells=L, vertices=v.shape[0], triangles=e.shape[0]))
 
