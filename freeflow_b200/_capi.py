@@ -25,10 +25,15 @@ STATUS_LINK_OVERFLOW = 2
 STATUS_FORCE_RANGE = 4
 STATUS_BAD_ELEMENT = 8
 
+# fixed scratch of ffs_lbm_step_noalloc
+NOALLOC_MAX_VERTICES = 32768
+NOALLOC_MAX_LINK_CELLS = 16384
+
 # every entry point include/ffs_lbm.h declares
 EXPORTS = (
     "ffs_lbm_create", "ffs_lbm_destroy", "ffs_lbm_set_flags", "ffs_lbm_get_flags", "ffs_lbm_initialize",
     "ffs_lbm_set_moments", "ffs_lbm_get_moments", "ffs_lbm_reserve_surface", "ffs_lbm_step",
+    "ffs_lbm_step_noalloc",
     "ffs_lbm_fill_solid", "ffs_lbm_get_status", "ffs_lbm_get_info", "ffs_lbm_debug_links",
     "ffs_lbm_profile_enable", "ffs_lbm_profile_read",
     "ffs_status_string", "ffs_last_error", "ffs_abi_version",
@@ -88,6 +93,7 @@ def load():
         "ffs_lbm_get_moments": [vp, vp, i32, i32, i32, vp],
         "ffs_lbm_reserve_surface": [vp, i32, i32],
         "ffs_lbm_step": [vp, C.POINTER(Surface), vp],
+        "ffs_lbm_step_noalloc": [vp, C.POINTER(Surface), vp],
         "ffs_lbm_fill_solid": [vp, C.POINTER(Surface), vp],
         "ffs_lbm_get_status": [vp, C.POINTER(C.c_uint32), i32, vp],
         "ffs_lbm_get_info": [vp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_double),

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -631,3 +632,131 @@ ffs_status ffs_lbm_profile_read(ffs_lbm *h, ffs_profile *out, int reset)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// ffs_lbm_step_noalloc: ffs_lbm_step with its moving-boundary scratch (link
+// table and per-vertex force accumulators) in a fixed device array of this
+// library instead of memory from cudaMalloc.  It allocates nothing, ever: no
+// cudaMalloc/cudaFree, no pool or library allocation.
+//
+// Callers that cannot allocate while stepping:
+//  * hosts that reserved their device memory up front and admitted work
+//    against that budget (a serving process packing many episodes into HBM,
+//    or a caller whose pool allocator already holds the free memory): a
+//    cudaMalloc in mid-run can fail with out-of-memory there;
+//  * latency-bound step loops that share the device with other streams:
+//    cudaMalloc/cudaFree synchronise the whole device and stall them.
+// ffs_lbm_step allocates its scratch on the first step with a surface (and
+// again for a larger one); this entry point never does.
+//
+// Scratch layout (one array shared by every grid and every call on a device):
+//   keys  [kNoallocSlots]  u32, 0 = empty slot          must start at 0
+//   list  [kNoallocSlots]  u32, claimed slots            no requirement
+//   count u32 (own 256-byte line)                        must start at 0
+//   links [kNoallocSlots * Q] u64, ~0 = no link          must start at ~0
+//   acc   [kNoallocMaxVertices * DIM] i64 force sums     must start at 0
+// Every call clears all four on its stream before its first kernel, so a
+// call never depends on the previous one having finished cleanly.  Calls
+// that overlap in time on one device (two streams, two threads, two grids)
+// race on the array: the caller orders them.
+namespace {
+
+constexpr uint32_t kNoallocSlots = 16384;       // link cells per step at most
+constexpr uint32_t kNoallocMaxVertices = 32768; // surface vertices at most
+constexpr size_t kNoallocKeysOff = 0;
+constexpr size_t kNoallocListOff = kNoallocKeysOff + sizeof(uint32_t) * kNoallocSlots;
+constexpr size_t kNoallocCountOff = kNoallocListOff + sizeof(uint32_t) * kNoallocSlots;
+constexpr size_t kNoallocLinksOff = kNoallocCountOff + 256;
+constexpr size_t kNoallocAccOff = kNoallocLinksOff + sizeof(unsigned long long) * kNoallocSlots * 27;
+constexpr size_t kNoallocBytes = kNoallocAccOff + sizeof(long long) * kNoallocMaxVertices * 3; // 4,456,704
+static_assert(kNoallocLinksOff % 256 == 0 && kNoallocAccOff % 256 == 0, "scratch sections stay 256-byte aligned");
+static_assert((kNoallocSlots & (kNoallocSlots - 1)) == 0, "the link table wants a power-of-two slot count");
+
+constexpr int kNoallocMaxDevices = 64;
+
+} // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_base[kNoallocMaxDevices] = {};
+
+// Address of the scratch array on the current device, looked up once per
+// device (the lookup may load this library's device code on that device).
+ffs_status noalloc_scratch(unsigned char **out)
+{
+    int dev = -1;
+    FFS_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) return fail(FFS_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        unsigned char *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(FFS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_base[dev] = p;
+    }
+    *out = g_noalloc_base[dev];
+    return FFS_OK;
+}
+
+template <int DIM, typename T> ffs_status noalloc_impl(ffs_lbm *h, const ffs_surface *s, unsigned char *base,
+                                                       cudaStream_t st)
+{
+    constexpr int Q = Lattice<DIM>::Q;
+    GridArgs<T> g = args<T>(h);
+    const bool surf = s && s->num_elements > 0;
+    SurfaceArgs sa = surface_args(s);
+    StepScalars sc{h->cl, h->ct, h->cf};
+    uint32_t *words = reinterpret_cast<uint32_t *>(h->flags);
+    LinkTable lt;
+    if (surf) {
+        lt.cap = kNoallocSlots;
+        lt.keys = reinterpret_cast<uint32_t *>(base + kNoallocKeysOff);
+        lt.list = reinterpret_cast<uint32_t *>(base + kNoallocListOff);
+        lt.count = reinterpret_cast<uint32_t *>(base + kNoallocCountOff);
+        lt.links = reinterpret_cast<unsigned long long *>(base + kNoallocLinksOff);
+        lt.acc = reinterpret_cast<long long *>(base + kNoallocAccOff);
+        lt.acc_cap = kNoallocMaxVertices;
+        FFS_CK(cudaMemsetAsync(base, 0, kNoallocLinksOff, st)); // keys, list, count
+        FFS_CK(cudaMemsetAsync(lt.links, 0xFF, sizeof(unsigned long long) * kNoallocSlots * Q, st));
+        FFS_CK(cudaMemsetAsync(lt.acc, 0, sizeof(long long) * (size_t)s->num_vertices * DIM, st));
+        FFS_CK((launch_detect_links<DIM, T>(g, words, lt, sa, sc, st)));
+    }
+    if (DIM == 2) FFS_CK(launch_dense2d<T>(g, st));
+    else FFS_CK(launch_dense3d<T>(g, st, h->dense_variant < 0 ? 0 : h->dense_variant));
+    if (surf) {
+        FFS_CK((launch_link_cells<DIM, T>(g, words, lt, sa, sc, st)));
+        FFS_CK(launch_finalize_forces<DIM>(lt, sa, h->cf, st));
+    }
+    h->cur ^= 1;
+    return FFS_OK;
+}
+
+template <int DIM> ffs_status noalloc_dim(ffs_lbm *h, const ffs_surface *s, unsigned char *base, cudaStream_t st)
+{
+    switch (h->d.storage) {
+    case FFS_STORAGE_F32: return noalloc_impl<DIM, float>(h, s, base, st);
+    case FFS_STORAGE_F16: return noalloc_impl<DIM, __half>(h, s, base, st);
+    default: return noalloc_impl<DIM, __nv_bfloat16>(h, s, base, st);
+    }
+}
+
+} // namespace
+
+extern "C" ffs_status ffs_lbm_step_noalloc(ffs_lbm *h, const ffs_surface *s, void *stream)
+{
+    if (!h) return fail(FFS_ERR_INVALID_ARGUMENT, "null grid");
+    ffs_status r = check_surface(h, s);
+    if (r != FFS_OK) return r;
+    if (s && s->num_elements > 0 && (uint32_t)s->num_vertices > kNoallocMaxVertices)
+        return fail(FFS_ERR_CAPACITY, "ffs_lbm_step_noalloc: " + std::to_string(s->num_vertices) +
+                                          " surface vertices exceed its fixed scratch (at most " +
+                                          std::to_string(kNoallocMaxVertices) + "); use ffs_lbm_step");
+    unsigned char *base = nullptr;
+    r = noalloc_scratch(&base);
+    if (r != FFS_OK) return r;
+    return h->dim == 2 ? noalloc_dim<2>(h, s, base, S(stream)) : noalloc_dim<3>(h, s, base, S(stream));
+}

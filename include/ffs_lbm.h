@@ -140,6 +140,24 @@ ffs_status ffs_lbm_reserve_surface(ffs_lbm *grid, int max_vertices, int max_link
  * Asynchronous on `stream`; no host synchronisation. */
 ffs_status ffs_lbm_step(ffs_lbm *grid, const ffs_surface *surface, void *stream);
 
+/* No counterpart in the reference.  The same step as ffs_lbm_step, with the
+ * same results, but it allocates no device memory: its link table and force
+ * accumulators live in one fixed array inside this library (4,456,704 bytes
+ * per device), for callers that must not allocate while stepping (a fixed,
+ * pre-reserved device-memory budget; loops that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree).
+ * Limits: at most FFS_NOALLOC_MAX_VERTICES surface vertices (larger surfaces
+ * return FFS_ERR_CAPACITY before any work); at most FFS_NOALLOC_MAX_LINK_CELLS
+ * cells may own links in one step (more latch status bit 2, link table
+ * overflow, like ffs_lbm_step with a too-small reservation).
+ * The first call on a device looks the array up on that device (set-up): make
+ * it before any stream capture.  Every call on a device shares the array and
+ * clears it on `stream` first, so calls that overlap in time on one device
+ * race: the caller orders them (one stream, or events). */
+#define FFS_NOALLOC_MAX_VERTICES 32768
+#define FFS_NOALLOC_MAX_LINK_CELLS 16384
+ffs_status ffs_lbm_step_noalloc(ffs_lbm *grid, const ffs_surface *surface, void *stream);
+
 /* fsi_coupling::fillSolidFlags2D (FsiCoupling2D.cu:434-464): Fluid cells
  * whose centre lies inside the closed polygon become SolidDynamic, and
  * SolidDynamic cells outside it return to Fluid.  dim == 2 only. */
