@@ -39,6 +39,13 @@ from freeflow_b200 import workloads as W  # noqa: E402
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
+# DRAM bytes (read + write) per cell of the dense kernel from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum), scaled to a launch by the
+# cells it processes; the capture and its command are in the named profile.
+DENSE_TRAFFIC_PER_CELL = {
+    (3, "f32"): (74.68, "profiles/launches_D3Q27_384x192x192_swimmer_f32.md"),
+}
+
 
 def algorithmic_bytes_per_cell(dim: int, storage: str) -> int:
     """2 * NM * s + 1: read and write NM moments of s bytes, read one flag byte."""
@@ -371,6 +378,9 @@ def run_ours(args):
     dense_avg_s = dense_ms * 1e-3 / max(1, dense_n)
     achieved = wl.ncell * bpc / dense_avg_s / 1e9
     launches_per_step = 1 + (3 if surf is not None else 0)
+    tpc = DENSE_TRAFFIC_PER_CELL.get((wl.dim, storage))
+    traffic = round(tpc[0] * wl.ncell) if tpc else None
+    traffic_src = f"{tpc[0]} B/cell measured by ncu, scaled to {wl.ncell} cells ({tpc[1]})" if tpc else None
     out = None
     if rank == 0:
         cpu = None
@@ -392,7 +402,8 @@ def run_ours(args):
                        "l2": "moment buffers exceed L2 (no flush needed)" if wl.ncell * bpc > 2 * 126e6
                        else "inputs smaller than L2", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
+                         "peak_kind": peak_kind,
                          "kernel": "dense3d_kernel" if wl.dim == 3 else "dense2d_kernel",
                          "bytes_per_cell": bpc, "kernel_ms": round(dense_ms / max(1, dense_n), 4)},
             "stages_ms_per_step": {k: round(v[0] / max(1, v[1]), 4) for k, v in prof.items() if v[1]},
