@@ -247,6 +247,110 @@ def run_reference(args):
     return 0
 
 
+
+# ---------------------------------------------------------------- serving
+def serving_velocity_error(storage: str, control_steps: int = 20, sides: str = "walls"):
+    """Relative L2 velocity error of a pool episode (256x128 swimmer) against
+    the FP64 oracle run on the same surfaces, after `control_steps` x 10 substeps."""
+    from freeflow_b200 import serving as S
+    from oracle.oracle import Oracle
+
+    sp = S.make_episode(256, 128, seed=51, length=control_steps, sides=sides)
+    pool = S.Pool(storage=storage, budget_bytes=256 << 20, max_episodes=2)
+    slot = pool.admit(sp)
+    o = Oracle(2, sp.nx, sp.ny, 1, viscosity=sp.viscosity, density=sp.density, dx=sp.dx, dt=sp.dt,
+               boundary_velocities=[0, 0, 0, 0], periodic=0, precision="phys64")
+    o.set_flags(sp.flags)
+    o.set_moments(pool.get_moments(slot).astype(np.float64))
+    q = 0
+    for c in range(control_steps):
+        a = np.random.default_rng(c).uniform(-1, 1, 8).astype(np.float32)
+        pool.set_action(slot, a)
+        pool.advance()
+        for _ in range(pool.substeps):
+            V, U = S.swimmer_surface(sp, a, q)
+            o.step(V, U, sp.elements, None)
+            q += 1
+    g = pool.get_moments(slot).astype(np.float64)
+    ref = o.get_moments()
+    err = float(np.linalg.norm(g[:, 1:3] - ref[:, 1:3]) / np.linalg.norm(ref[:, 1:3]))
+    o.close()
+    pool.close()
+    return err
+
+
+def run_serving(iterations: int, warmup: int, concurrency: int = 256, plain_steps: int = 20, seed: int = 0):
+    """Config E: Poisson stream of 2D swimmer episodes (grids uniform over
+    256x128, 512x192, 1200x400; 8 actions per control step; 10 substeps per
+    action; lengths uniform in 200..2000 control steps) through the FP16 pool
+    with continuous batching, against the plain per-episode FP32 path."""
+    import torch
+    from freeflow_b200 import serving as S
+
+    mean_len = 1100.0
+    per_iter = concurrency / mean_len
+    n_specs = concurrency + int(per_iter * (iterations + warmup) * 1.5) + 16
+    specs = S.serving_mix(n_specs, seed=seed)
+    pool = S.Pool(storage="f16", budget_bytes=6 << 30, max_episodes=2 * concurrency, substeps=10, num_actions=8)
+    t0 = time.perf_counter()
+    r = S.serve(pool, specs, iterations=iterations, initial=concurrency, arrivals_per_iter=per_iter, seed=seed,
+                warmup_iterations=warmup)
+    info = r.pop("pool_info_at_end")
+    pool.close()
+    torch.cuda.synchronize()
+    # plain path: one episode of each grid size, one at a time
+    sample = [S.make_episode(nx, ny, seed=1000 + i, length=plain_steps) for i, (nx, ny) in enumerate(S.SERVING_SIZES)]
+    plain = S.plain_rate(sample, plain_steps)
+    peak, peak_kind = hbm_peak()
+    dense_gbs = info["tuned_cells"] * 25 / (info["dense_ms"] * 1e-3) / 1e9 if info["dense_ms"] > 0 else None
+    out = {
+        "workload": "E: D2Q9 swimmer mix {256x128, 512x192, 1200x400}, 198-edge fish, 8 actions x 10 substeps",
+        "storage": "f16",
+        "batched": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()},
+        "plain_f32": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in plain.items()},
+        "speedup_vs_plain": round(r["env_steps_per_s"] / plain["env_steps_per_s"], 2),
+        "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}", "graph_builds": info["graph_builds"],
+                 "max_episodes": 2 * concurrency,
+                 "dense_ms_at_tuning": round(info["dense_ms"], 4), "cells_at_tuning": info["tuned_cells"],
+                 "dense_roofline": ({"achieved": round(dense_gbs, 1), "peak": peak, "unit": "GB/s",
+                                     "frac": round(dense_gbs / peak, 4), "bytes_per_cell": 25,
+                                     "peak_kind": peak_kind} if dense_gbs else None)},
+        "velocity_rel_err_vs_fp64": {
+            "closed_tank": {"f16": serving_velocity_error("f16"), "f32": serving_velocity_error("f32")},
+            "outlets": {"f16": serving_velocity_error("f16", sides="outlets"),
+                        "f32": serving_velocity_error("f32", sides="outlets")},
+            "case": "256x128 swimmer, 200 substeps, same surfaces as the FP64 oracle; with outlets the "
+                    "reference's sign-switched outlet rule makes even FP32 differ from FP64 (branch flips)"},
+        "seconds": round(time.perf_counter() - t0, 1),
+    }
+    return out
+
+
+def run_serving_line(args):
+    """`--workload E`: the serving measurement as its own JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    r = run_serving(iterations=args.steps, warmup=args.warmup)
+    b = r["batched"]
+    line = {
+        "metric": "env_steps_per_s", "value": b["env_steps_per_s"], "unit": "env-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * b["seconds"] / max(1, args.steps), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16", "data": "synthetic (seeded)",
+        "config": {"workload": r["workload"], "storage": "f16", "concurrency_mean": b["concurrency_mean"],
+                   "l2": "episode state exceeds L2 at this concurrency"},
+        "p50_ms": b["p50_ms"], "p99_ms": b["p99_ms"],
+        # per control step the pool uploads one 576-byte parameter row per episode
+        # and reads back the 48-byte output records of all its slots
+        "e2e": {"value": b["env_steps_per_s"], "unit": "env-steps/s", "h2d_bytes_per_step": 576,
+                "d2h_bytes_per_step": round(48 * r["pool"]["max_episodes"] / max(1.0, b["concurrency_mean"]), 1)},
+        "serving": r,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------- GPU
 def run_ours(args):
     import torch
@@ -413,6 +517,8 @@ def run_ours(args):
             "clocks": clk,
             "device_status": status,
         }
+        if world == 1 and not args.no_serving and not args.small:
+            out["serving"] = run_serving(iterations=150, warmup=20)
         print(json.dumps(out), flush=True)
     g.close()
     if world > 1:
@@ -427,15 +533,18 @@ def main():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="D", choices=["A", "B", "C", "D"])
+    p.add_argument("--workload", default="D", choices=["A", "B", "C", "D", "E"])
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     p.add_argument("--small", action="store_true", help="reduced grid (profiling captures)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving (config E) sub-measurement")
     args = p.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "E":
+        return run_serving_line(args)
     return run_ours(args)
 
 

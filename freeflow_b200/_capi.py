@@ -29,7 +29,7 @@ STATUS_BAD_ELEMENT = 8
 NOALLOC_MAX_VERTICES = 32768
 NOALLOC_MAX_LINK_CELLS = 16384
 
-# every entry point include/ffs_lbm.h declares
+# every entry point include/ffs_lbm.h and include/ffs_pool.h declare
 EXPORTS = (
     "ffs_lbm_create", "ffs_lbm_destroy", "ffs_lbm_set_flags", "ffs_lbm_get_flags", "ffs_lbm_initialize",
     "ffs_lbm_set_moments", "ffs_lbm_get_moments", "ffs_lbm_reserve_surface", "ffs_lbm_step",
@@ -37,6 +37,9 @@ EXPORTS = (
     "ffs_lbm_fill_solid", "ffs_lbm_get_status", "ffs_lbm_get_info", "ffs_lbm_debug_links",
     "ffs_lbm_profile_enable", "ffs_lbm_profile_read",
     "ffs_status_string", "ffs_last_error", "ffs_abi_version",
+    "ffs_pool_create", "ffs_pool_destroy", "ffs_pool_episode_bytes", "ffs_pool_admit", "ffs_pool_evict",
+    "ffs_pool_set_action", "ffs_pool_advance", "ffs_pool_collect", "ffs_pool_get_moments", "ffs_pool_tune",
+    "ffs_pool_get_info", "ffs_swimmer_surface",
 )
 
 
@@ -65,6 +68,38 @@ class Surface(C.Structure):
         ("forces", C.c_void_p), ("forces64", C.c_void_p),
     ]
 
+
+class PoolDesc(C.Structure):
+    _fields_ = [("storage", C.c_int), ("budget_bytes", C.c_int64), ("max_episodes", C.c_int),
+                ("substeps", C.c_int), ("num_actions", C.c_int), ("max_link_cells", C.c_int),
+                ("stream", C.c_void_p)]
+
+
+class Swimmer(C.Structure):
+    _fields_ = [("num_vertices", C.c_int), ("num_elements", C.c_int),
+                ("rest", C.c_void_p), ("elements", C.c_void_p), ("amplitude", C.c_void_p),
+                ("sin_kx", C.c_void_p), ("cos_kx", C.c_void_p), ("segment", C.c_void_p),
+                ("omega", C.c_double), ("t0", C.c_double)]
+
+
+class EpisodeDesc(C.Structure):
+    _fields_ = [("grid", LbmDesc), ("flags", C.c_void_p), ("swimmer", Swimmer)]
+
+
+class PoolOutput(C.Structure):
+    _fields_ = [("energy", C.c_double), ("force", C.c_double * 2), ("torque", C.c_double),
+                ("status", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class PoolInfo(C.Structure):
+    _fields_ = [("budget_bytes", C.c_int64), ("free_bytes", C.c_int64), ("largest_free_bytes", C.c_int64),
+                ("active_episodes", C.c_int), ("tiles", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int),
+                ("advances", C.c_int64), ("graph_builds", C.c_int64), ("cells", C.c_int64),
+                ("tuned_cells", C.c_int64), ("dense_ms", C.c_double)]
+
+
+POOL_MAX_ACTIONS = 16
+POOL_MAX_SUBSTEPS = 64
 
 _LIB = None
 
@@ -101,6 +136,18 @@ def load():
         "ffs_lbm_debug_links": [vp, C.POINTER(Surface), vp, vp, i64, C.POINTER(i64), vp],
         "ffs_lbm_profile_enable": [vp, i32],
         "ffs_lbm_profile_read": [vp, C.POINTER(Profile), i32],
+        "ffs_pool_create": [C.POINTER(PoolDesc), C.POINTER(vp)],
+        "ffs_pool_destroy": [vp],
+        "ffs_pool_episode_bytes": [vp, C.POINTER(EpisodeDesc), C.POINTER(i64)],
+        "ffs_pool_admit": [vp, C.POINTER(EpisodeDesc), C.POINTER(i32)],
+        "ffs_pool_evict": [vp, i32],
+        "ffs_pool_set_action": [vp, i32, vp, i32],
+        "ffs_pool_advance": [vp],
+        "ffs_pool_collect": [vp, i32, C.POINTER(PoolOutput), vp],
+        "ffs_pool_get_moments": [vp, i32, vp],
+        "ffs_pool_tune": [vp],
+        "ffs_pool_get_info": [vp, C.POINTER(PoolInfo)],
+        "ffs_swimmer_surface": [C.POINTER(Swimmer), vp, i32, i64, C.c_double, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -1,0 +1,321 @@
+// Batched D2Q9 kernels of the serving pool: every kernel covers all admitted
+// episodes of the pool in one launch.
+//
+// Work items are numbered across episodes through the prefix sums of the
+// active table (dense tiles, surface elements, surface vertices); an item
+// finds its episode by a binary search over at most kPoolMaxSlots prefixes.
+// The per-item bodies are the single-grid ones (dense2d_tile, detect_pair,
+// link_cell_update), so a pool episode computes bit for bit what the same
+// grid computes alone through ffs_lbm_step.  The grids are persistent
+// (a fixed number of CTAs striding over a count read from device memory), so
+// one captured CUDA graph serves every mix of episodes.
+//
+// Reference: one Simulator2D per environment process, each step through
+// fsi_coupling::solveLbmAndFsiStep2D (src/core/FsiCoupling2D.cu:358-432);
+// the environment loop is rl/env.py:163-217.
+#include "ffs_links_dev.cuh"
+#include "ffs_pool.cuh"
+
+namespace fflbm {
+
+namespace {
+
+// Index of the active entry whose range [prefix[i], prefix[i+1]) holds t.
+__device__ __forceinline__ int owner_of(const uint32_t *prefix, int n, uint32_t t)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename T> __device__ __forceinline__ GridArgs<T> episode_args(const PoolEpisode &e, int parity)
+{
+    GridArgs<T> g;
+    g.nx = e.nx;
+    g.ny = e.ny;
+    g.nz = 1;
+    g.ncell = e.ncell;
+    g.periodic = 0;
+    g.half_pops = 0;
+    g.omega = e.omega;
+    g.codec = e.codec;
+    g.src = static_cast<const T *>(e.mom[parity]);
+    g.dst = static_cast<T *>(e.mom[parity ^ 1]);
+    g.flags = e.flags;
+    g.wallmask = e.wallmask;
+    g.status = e.status;
+    return g;
+}
+
+__device__ __forceinline__ SurfaceArgs episode_surface(const PoolEpisode &e)
+{
+    SurfaceArgs s;
+    s.V = e.V;
+    s.U = e.U;
+    s.E = e.elements;
+    s.nv = e.nv;
+    s.ne = e.ne;
+    s.forces = nullptr;
+    s.forces64 = nullptr;
+    return s;
+}
+
+} // namespace
+
+// ------------------------------------------------------------ kinematics
+__global__ void pool_kinematics_kernel(const PoolEpisode *eps, const PoolParams *prm, const PoolActive *act,
+                                       int substep)
+{
+    const int n = (int)act->n;
+    if (n == 0) return;
+    const uint32_t total = act->vert_prefix[n];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int a = owner_of(act->vert_prefix, n, t);
+        const uint32_t s = act->slot[a];
+        const PoolEpisode &e = eps[s];
+        const PoolParams &p = prm[a];
+        const uint32_t v = t - act->vert_prefix[a];
+        float x, y, vx, vy;
+        swimmer_vertex(e.rest[2 * v], e.rest[2 * v + 1], e.amp[v], e.sin_kx[v], e.cos_kx[v], e.segment[v], p.actions,
+                       p.sb[substep], p.cb[substep], e.wave_omega, x, y, vx, vy);
+        e.V[2 * v] = x;
+        e.V[2 * v + 1] = y;
+        e.U[2 * v] = vx;
+        e.U[2 * v + 1] = vy;
+    }
+}
+
+// ---------------------------------------------------------------- detect
+template <typename T>
+__global__ void pool_detect_kernel(const PoolEpisode *eps, const PoolActive *act, LinkTable lt, uint32_t *owner,
+                                   int parity)
+{
+    const int n = (int)act->n;
+    if (n == 0) return;
+    const long long total = (long long)act->elem_prefix[n] * 8;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
+         p += (long long)gridDim.x * blockDim.x) {
+        const uint32_t ge = (uint32_t)(p >> 3);
+        const int l = (int)(p & 7) + 1;
+        const int a = owner_of(act->elem_prefix, n, ge);
+        const uint32_t s = act->slot[a];
+        const PoolEpisode &e = eps[s];
+        const GridArgs<T> g = episode_args<T>(e, parity);
+        const SurfaceArgs sa = episode_surface(e);
+        const StepScalars sc{e.cl, e.ct, e.cf};
+        detect_pair<2, T>(g, reinterpret_cast<uint32_t *>(e.flags), lt, sa, sc, (long long)(ge - act->elem_prefix[a]),
+                          l, e.cell_base, owner, s);
+    }
+}
+
+// ----------------------------------------------------------------- dense
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
+{
+    __shared__ float sp[9][TY + 2][TX + 2];
+    const int n = (int)act->n;
+    if (n == 0) return;
+    const uint32_t total = act->tile_prefix[n];
+    for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const int a = owner_of(act->tile_prefix, n, t);
+        const uint32_t local = t - act->tile_prefix[a];
+        const uint32_t tx = local % act->tiles_x[a], ty = local / act->tiles_x[a];
+        const GridArgs<T> g = episode_args<T>(eps[act->slot[a]], parity);
+        dense2d_tile<T, false, TX, TY>(g, (int)tx * TX, (int)ty * TY, sp);
+        __syncthreads(); // the next tile reuses sp
+    }
+}
+
+// ------------------------------------------------------------ link cells
+template <typename T>
+__global__ void __launch_bounds__(256, 3) pool_link_cells_kernel(const PoolEpisode *eps, LinkTable lt,
+                                                                 const uint32_t *owner, int parity)
+{
+    constexpr int Q = 9;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t n = *lt.count;
+    for (uint32_t w = ((blockIdx.x * blockDim.x) + threadIdx.x) >> 5; w < n; w += nwarps) {
+        const uint32_t slot = lt.list[w];
+        const PoolEpisode &e = eps[owner[slot]];
+        const uint32_t cell = lt.keys[slot] - 1 - e.cell_base;
+        const GridArgs<T> g = episode_args<T>(e, parity);
+        const SurfaceArgs sa = episode_surface(e);
+        const StepScalars sc{e.cl, e.ct, e.cf};
+        link_cell_update<2, T, false>(g, lt.links, slot, cell, e.acc, sa, sc);
+        if (lane < Q) lt.links[(size_t)slot * Q + lane] = ~0ull;
+        __syncwarp();
+        if (lane == 0) {
+            lt.keys[slot] = 0;
+            set_link_bit(reinterpret_cast<uint32_t *>(e.flags), cell, false);
+        }
+    }
+}
+
+// -------------------------------------------------------------- finalize
+// One CTA per active episode: scales the fixed-point sums to forces, clears
+// them, and reduces total force, torque and power in a fixed order (so the
+// sums do not depend on the mix or on launch order).
+__global__ void __launch_bounds__(256) pool_finalize_kernel(const PoolEpisode *eps, const PoolActive *act,
+                                                            LinkTable lt)
+{
+    __shared__ double red[4][8];
+    const int n = (int)act->n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *lt.count = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int a = blockIdx.x; a < n; a += gridDim.x) {
+        const PoolEpisode &e = eps[act->slot[a]];
+        double fx = 0.0, fy = 0.0, tq = 0.0, pw = 0.0;
+        for (int v = threadIdx.x; v < e.nv; v += blockDim.x) {
+            // the single-grid finalize's expression (finalize_forces_kernel)
+            const double f0 = (double)e.acc[2 * v] * (1.0 / kForceScale) * e.cf;
+            const double f1 = (double)e.acc[2 * v + 1] * (1.0 / kForceScale) * e.cf;
+            e.acc[2 * v] = 0;
+            e.acc[2 * v + 1] = 0;
+            e.force[2 * v] = f0;
+            e.force[2 * v + 1] = f1;
+            const double rx = (double)e.V[2 * v] - (double)e.cx0, ry = (double)e.V[2 * v + 1] - (double)e.cy0;
+            fx += f0;
+            fy += f1;
+            tq += rx * f1 - ry * f0;
+            pw -= f0 * (double)e.U[2 * v] + f1 * (double)e.U[2 * v + 1];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            fx += __shfl_xor_sync(0xffffffffu, fx, o);
+            fy += __shfl_xor_sync(0xffffffffu, fy, o);
+            tq += __shfl_xor_sync(0xffffffffu, tq, o);
+            pw += __shfl_xor_sync(0xffffffffu, pw, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = fx;
+            red[1][warp] = fy;
+            red[2][warp] = tq;
+            red[3][warp] = pw;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                for (int k = 0; k < 4; ++k) s[k] += red[k][w];
+            // rl/env.py:172-175: energy += power * dt when the power is positive
+            if (s[3] > 0.0) e.sums[0] += s[3] * (double)e.ct;
+            e.sums[1] += s[0];
+            e.sums[2] += s[1];
+            e.sums[3] += s[2];
+        }
+        __syncthreads();
+    }
+}
+
+// One thread per active episode: publish the control step's sums and the
+// latched status, then clear them for the next control step.
+__global__ void pool_outputs_kernel(const PoolEpisode *eps, const PoolActive *act, PoolOutput *out, int substeps)
+{
+    const int n = (int)act->n;
+    const double inv = 1.0 / (double)substeps;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        const uint32_t s = act->slot[a];
+        const PoolEpisode &e = eps[s];
+        PoolOutput o;
+        o.energy = e.sums[0];
+        o.force[0] = e.sums[1] * inv;
+        o.force[1] = e.sums[2] * inv;
+        o.torque = e.sums[3] * inv;
+        o.status = *e.status;
+        o.pad = 0;
+        out[s] = o;
+        for (int k = 0; k < 4; ++k) e.sums[k] = 0.0;
+        *e.status = 0;
+    }
+}
+
+// -------------------------------------------------------------- launchers
+cudaError_t launch_pool_kinematics(const PoolEpisode *eps, const PoolParams *prm, const PoolActive *act, int substep,
+                                   int grid, cudaStream_t st)
+{
+    pool_kinematics_kernel<<<grid, 256, 0, st>>>(eps, prm, act, substep);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_pool_detect(const PoolEpisode *eps, const PoolActive *act, const LinkTable &lt, uint32_t *owner,
+                               int parity, int grid, cudaStream_t st)
+{
+    pool_detect_kernel<T><<<grid, 128, 0, st>>>(eps, act, lt, owner, parity);
+    return cudaGetLastError();
+}
+
+template <typename T, int TX, int TY> static const void *dense_fn()
+{
+    return reinterpret_cast<const void *>(&pool_dense_kernel<T, TX, TY>);
+}
+
+template <typename T>
+cudaError_t launch_pool_dense(const PoolEpisode *eps, const PoolActive *act, int parity, int shape, int grid,
+                              cudaStream_t st)
+{
+    switch (shape) {
+    case 0: pool_dense_kernel<T, 32, 4><<<grid, 32 * 4, 0, st>>>(eps, act, parity); break;
+    case 1: pool_dense_kernel<T, 32, 8><<<grid, 32 * 8, 0, st>>>(eps, act, parity); break;
+    case 2: pool_dense_kernel<T, 64, 4><<<grid, 64 * 4, 0, st>>>(eps, act, parity); break;
+    case 3: pool_dense_kernel<T, 32, 16><<<grid, 32 * 16, 0, st>>>(eps, act, parity); break;
+    default: pool_dense_kernel<T, 64, 8><<<grid, 64 * 8, 0, st>>>(eps, act, parity); break;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T> int pool_dense_blocks_per_sm(int shape)
+{
+    const void *fn;
+    int threads;
+    switch (shape) {
+    case 0: fn = dense_fn<T, 32, 4>(); threads = 128; break;
+    case 1: fn = dense_fn<T, 32, 8>(); threads = 256; break;
+    case 2: fn = dense_fn<T, 64, 4>(); threads = 256; break;
+    case 3: fn = dense_fn<T, 32, 16>(); threads = 512; break;
+    default: fn = dense_fn<T, 64, 8>(); threads = 512; break;
+    }
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, 0) != cudaSuccess || blocks < 1) blocks = 1;
+    return blocks;
+}
+
+template <typename T>
+cudaError_t launch_pool_link_cells(const PoolEpisode *eps, const LinkTable &lt, const uint32_t *owner, int parity,
+                                   int grid, cudaStream_t st)
+{
+    pool_link_cells_kernel<T><<<grid, 256, 0, st>>>(eps, lt, owner, parity);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pool_finalize(const PoolEpisode *eps, const PoolActive *act, const LinkTable &lt, int grid,
+                                 cudaStream_t st)
+{
+    pool_finalize_kernel<<<grid, 256, 0, st>>>(eps, act, lt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pool_outputs(const PoolEpisode *eps, const PoolActive *act, PoolOutput *out, int substeps,
+                                cudaStream_t st)
+{
+    pool_outputs_kernel<<<(kPoolMaxSlots + 127) / 128, 128, 0, st>>>(eps, act, out, substeps);
+    return cudaGetLastError();
+}
+
+#define FFS_INST_POOL(T)                                                                                               \
+    template cudaError_t launch_pool_detect<T>(const PoolEpisode *, const PoolActive *, const LinkTable &, uint32_t *, \
+                                               int, int, cudaStream_t);                                                \
+    template cudaError_t launch_pool_dense<T>(const PoolEpisode *, const PoolActive *, int, int, int, cudaStream_t);   \
+    template int pool_dense_blocks_per_sm<T>(int);                                                                     \
+    template cudaError_t launch_pool_link_cells<T>(const PoolEpisode *, const LinkTable &, const uint32_t *, int, int, \
+                                                   cudaStream_t);
+FFS_INST_POOL(float)
+FFS_INST_POOL(__half)
+FFS_INST_POOL(__nv_bfloat16)
+
+} // namespace fflbm

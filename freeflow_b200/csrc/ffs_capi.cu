@@ -65,6 +65,15 @@ ffs_status fail(ffs_status s, const std::string &msg)
     return s;
 }
 
+} // namespace
+
+// Error reporting shared with the other C-ABI translation units (ffs_pool.cu).
+namespace fflbm {
+ffs_status record_error(ffs_status s, const std::string &msg) { return fail(s, msg); }
+} // namespace fflbm
+
+namespace {
+
 #define FFS_CK(expr)                                                                                                    \
     do {                                                                                                                \
         cudaError_t e_ = (expr);                                                                                        \

@@ -24,19 +24,20 @@ __device__ __forceinline__ int halo_index(int v, int n, bool wrap)
     return v;
 }
 
-// Processes the tile with lower-left cell (x0, y0).  The caller's CTA has
-// D2::kThreads threads; sp is the CTA's population tile.
-template <typename T, bool HALF>
-__device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y0, float (*sp)[D2::kHY][D2::kHX])
+// Processes the TX x TY tile with lower-left cell (x0, y0).  The caller's
+// CTA has TX * TY threads; sp is the CTA's population tile (tile + halo).
+template <typename T, bool HALF, int TX = D2::kTX, int TY = D2::kTY>
+__device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y0, float (*sp)[TY + 2][TX + 2])
 {
     using L = Lattice<2>;
+    constexpr int kHX = TX + 2, kHalo = (TX + 2) * (TY + 2), kThreads = TX * TY;
     const int tid = threadIdx.x;
     const bool wx = g.periodic & 1, wy = g.periodic & 2;
 
     // 1. reconstruct the tile + halo.  The halo index is clamped (the
     //    reference's min/max, FsiCoupling2D.cu:104-105) or wrapped (periodic).
-    for (int c = tid; c < D2::kHalo; c += D2::kThreads) {
-        int hx = c % D2::kHX, hy = c / D2::kHX;
+    for (int c = tid; c < kHalo; c += kThreads) {
+        int hx = c % kHX, hy = c / kHX;
         int gx = halo_index(x0 + hx - 1, g.nx, wx);
         int gy = halo_index(y0 + hy - 1, g.ny, wy);
         float m[6];
@@ -50,7 +51,7 @@ __device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y
     }
     __syncthreads();
 
-    const int tx = tid % D2::kTX, ty = tid / D2::kTX;
+    const int tx = tid % TX, ty = tid / TX;
     const int x = x0 + tx, y = y0 + ty;
     if (x < g.nx && y < g.ny) {
         const uint32_t idx = (uint32_t)(y * g.nx + x);

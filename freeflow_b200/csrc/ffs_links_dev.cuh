@@ -1,0 +1,303 @@
+// Device bodies of the moving-boundary stages, shared by the single-grid
+// kernels (ffs_links.cu) and the batched many-grid kernels (ffs_batch2d.cu).
+#pragma once
+#include "ffs_geom.cuh"
+#include "ffs_links.cuh"
+#include "ffs_math.cuh"
+#include "ffs_outlet.cuh"
+#include "ffs_dense2d.cuh"
+
+namespace fflbm {
+
+__device__ __forceinline__ uint32_t hash_cell(uint32_t c)
+{
+    c ^= c >> 16; c *= 0x7feb352dU; c ^= c >> 15; c *= 0x846ca68bU; c ^= c >> 16;
+    return c;
+}
+
+__device__ __forceinline__ void set_link_bit(uint32_t *flag_words, uint32_t cell, bool on)
+{
+    uint32_t bit = (uint32_t)kBitLink << (8 * (cell & 3));
+    if (on) atomicOr(flag_words + (cell >> 2), bit);
+    else atomicAnd(flag_words + (cell >> 2), ~bit);
+}
+
+// Finds or claims the cell's slot and keeps the smallest key of direction l.
+// The table key is key_base + cell + 1: one table can serve many grids whose
+// cells are numbered from distinct bases; the claiming thread tags the slot
+// with owner_id in `owner` when that array is given.
+template <int Q>
+__device__ __forceinline__ void insert_link(const LinkTable &lt, uint32_t *flag_words, uint32_t cell, int l,
+                                            unsigned long long key, uint32_t *status, uint32_t key_base = 0,
+                                            uint32_t *owner = nullptr, uint32_t owner_id = 0)
+{
+    const uint32_t tkey = key_base + cell + 1;
+    uint32_t slot = hash_cell(tkey - 1) & (lt.cap - 1);
+    for (uint32_t probe = 0; probe < lt.cap; ++probe) {
+        uint32_t cur = lt.keys[slot];
+        if (cur == 0) {
+            uint32_t old = atomicCAS(lt.keys + slot, 0u, tkey);
+            if (old == 0) {
+                uint32_t pos = atomicAdd(lt.count, 1u);
+                lt.list[pos] = slot;
+                if (owner) owner[slot] = owner_id;
+                set_link_bit(flag_words, cell, true);
+                cur = tkey;
+            } else {
+                cur = old;
+            }
+        }
+        if (cur == tkey) {
+            atomicMin(lt.links + (size_t)slot * Q + l, key);
+            return;
+        }
+        slot = (slot + 1) & (lt.cap - 1);
+    }
+    atomicOr(status, kStatusLinkOverflow);
+}
+
+// Link detection of element e in direction l (1 <= l < Q): every cell of
+// the element's bounding box grown by one cell whose link segment
+// x -> x - c_l crosses the element gets a (depth, element) key.
+template <int DIM, typename T>
+__device__ __forceinline__ void detect_pair(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt,
+                                            const SurfaceArgs &s, const StepScalars &sc, long long e, int l,
+                                            uint32_t key_base = 0, uint32_t *owner = nullptr,
+                                            uint32_t owner_id = 0)
+{
+    constexpr int Q = Lattice<DIM>::Q;
+    uint32_t vid[3] = {0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) {
+        vid[j] = s.E[DIM * e + j];
+        if (vid[j] >= (uint32_t)s.nv) { atomicOr(g.status, kStatusBadElement); return; }
+    }
+    // getBoundingBox: min from FLT_MAX, max from FLT_MIN (sic), then / dx
+    float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+    float bmax[3] = {1.175494351e-38f, 1.175494351e-38f, 1.175494351e-38f};
+#pragma unroll
+    for (int j = 0; j < DIM; ++j)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            float c = s.V[(size_t)vid[j] * DIM + k];
+            if (c < bmin[k]) bmin[k] = c;
+            if (bmax[k] < c) bmax[k] = c;
+        }
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    const int n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        lo[k] = max(__float2int_rz(geom::dvd(bmin[k], sc.cl)) - 1, 0);
+        hi[k] = min(__float2int_rz(geom::dvd(bmax[k], sc.cl)) + 1, n[k] - 1);
+    }
+    int cx, cy, cz;
+    dir_vec<DIM>(l, cx, cy, cz);
+    const float cl = sc.cl;
+    for (int k3 = lo[2]; k3 <= hi[2]; ++k3)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+                geom::Hit h;
+                if (DIM == 2) {
+                    h = geom::isect2(s.V, vid[0], vid[1], geom::mul((float)i, cl), geom::mul((float)j, cl),
+                                     geom::mul(geom::sub((float)i, (float)cx), cl),
+                                     geom::mul(geom::sub((float)j, (float)cy), cl));
+                } else {
+                    float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
+                    float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl),
+                                   geom::mul(geom::sub((float)j, (float)cy), cl),
+                                   geom::mul(geom::sub((float)k3, (float)cz), cl)};
+                    h = geom::isect3(s.V, vid[0], vid[1], vid[2], p1, p2);
+                }
+                if (!h.hit) continue;
+                const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
+                insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status, key_base,
+                               owner, owner_id);
+            }
+}
+
+// Per-vertex force shares of the links of one cell.  Lanes whose links hit
+// the same element (found with __match_any_sync) are summed with the warp's
+// integer reduction unit (__reduce_add_sync), one value per (vertex slot,
+// component), in 2^-24 fixed point; the group leader then adds each sum, in
+// 2^-32 fixed point, to the vertex accumulator with one 64-bit integer
+// atomic.  Integer sums are associative, so the per-vertex result does not
+// depend on warp, lane or launch order.  A share beyond +-127 lattice units
+// (outside the 2^-24 range of 27 summed int32 shares) is clamped and flagged.
+template <int DIM>
+__device__ __forceinline__ void add_forces_warp(long long *acc, bool active, uint32_t elem, const uint32_t *vert,
+                                                const float (*share)[3], uint32_t *status)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned peers = __match_any_sync(full, active ? elem : 0xffffffffu);
+    const int lane = threadIdx.x & 31;
+    const bool leader = active && lane == __ffs(peers) - 1;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j)
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            float v = active ? share[j][k] : 0.0f;
+            if (!(fabsf(v) < 127.0f)) {
+                if (active) atomicOr(status, kStatusForceRange);
+                v = isfinite(v) ? copysignf(127.0f, v) : 0.0f;
+            }
+            const int q = __float2int_rn(v * 16777216.0f); // 2^24
+            const int sum = (int)__reduce_add_sync(peers, (unsigned)q);
+            if (leader && sum != 0)
+                atomicAdd(reinterpret_cast<unsigned long long *>(acc + (size_t)vert[j] * DIM + k),
+                          (unsigned long long)((long long)sum * 256)); // 2^24 -> 2^32
+        }
+}
+
+// Update of one link-owning cell by one warp (lane i = direction i): wall
+// bounce-back, moving-wall reconstruction with its momentum-exchange force
+// shares, or the ordinary pull; the raw moments are reduced across the
+// warp and lane 0 collides, stores and feeds outlets.  `links` holds the
+// Q keys of the cell's table slot; the force shares go to `acc`.
+template <int DIM, typename T, bool HALF>
+__device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const unsigned long long *links,
+                                                 uint32_t slot, uint32_t cell, long long *acc,
+                                                 const SurfaceArgs &s, const StepScalars &sc)
+{
+    constexpr int Q = Lattice<DIM>::Q, NM = Lattice<DIM>::NM;
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const long long nxy = (long long)g.nx * g.ny;
+    const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
+    const int x = (int)(cell % g.nx);
+    const int y = (int)((cell / g.nx) % g.ny);
+    const int z = (int)(cell / nxy);
+    const uint8_t f8 = g.flags[cell];
+    if (is_updated(f8 & kTypeMask)) {
+        float mc[NM];
+        load_moments<DIM, T>(mc, g.src, g.ncell, cell, g.codec);
+        Coef<DIM> own;
+        own.make(mc);
+        float pop = 0.0f;
+        bool has_share = false;
+        uint32_t hit_elem = 0xffffffffu;
+        uint32_t vshare[3] = {0, 0, 0};
+        float share[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; // [vertex][component]
+        if (lane < Q) {
+            const int i = lane;
+            int cx, cy, cz;
+            dir_vec<DIM>(i, cx, cy, cz);
+            const int x1 = x - cx, y1 = y - cy, z1 = z - cz;
+            const bool notCross = x1 >= 0 && x1 < g.nx && y1 >= 0 && y1 < g.ny && z1 >= 0 && z1 < g.nz;
+            const int ax = (x1 + g.nx) % g.nx, ay = (y1 + g.ny) % g.ny, az = (z1 + g.nz) % g.nz;
+            const uint32_t ib = (uint32_t)((long long)az * nxy + (long long)ay * g.nx + ax);
+            bool done = false;
+            if (is_bounce_back<DIM>(g.flags[ib] & kTypeMask)) {
+                float v = own.population(-cx, -cy, -cz);
+                if (HALF) v = round_half(v);
+                pop = fmaxf(v, 0.0f);
+                done = true;
+            } else if (notCross) {
+                const unsigned long long key = links[(size_t)slot * Q + i];
+                if (key != ~0ull) {
+                    const uint32_t e = (uint32_t)(key & 0xffffffffull);
+                    const float cl = sc.cl;
+                    geom::Hit h;
+                    uint32_t vv[3] = {s.E[DIM * (size_t)e], s.E[DIM * (size_t)e + 1], DIM == 3 ? s.E[DIM * (size_t)e + 2] : 0u};
+                    if (DIM == 2) {
+                        h = geom::isect2(s.V, vv[0], vv[1], geom::mul((float)x, cl), geom::mul((float)y, cl),
+                                         geom::mul((float)x1, cl), geom::mul((float)y1, cl));
+                    } else {
+                        float p1[3] = {geom::mul((float)x, cl), geom::mul((float)y, cl), geom::mul((float)z, cl)};
+                        float p2[3] = {geom::mul((float)x1, cl), geom::mul((float)y1, cl), geom::mul((float)z1, cl)};
+                        h = geom::isect3(s.V, vv[0], vv[1], vv[2], p1, p2);
+                    }
+                    if (h.hit) {
+                        // wall velocity at the hit point, in lattice units
+                        float uw[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) {
+                            float a = s.U[(size_t)vv[0] * DIM + k] * h.b[0] + s.U[(size_t)vv[1] * DIM + k] * h.b[1];
+                            if (DIM == 3) a += s.U[(size_t)vv[2] * DIM + k] * h.b[2];
+                            uw[k] = (DIM == 2) ? a * (sc.ct / sc.cl) : (a * sc.ct) / sc.cl;
+                        }
+                        // moving-wall population: Hermite expansion with the cell's
+                        // density, the wall velocity and pi' = pi + uw uw - u u
+                        float mw[NM];
+                        mw[0] = mc[0];
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) mw[1 + k] = uw[k];
+#pragma unroll
+                        for (int k = DIM + 1; k < NM; ++k) {
+                            const int a = MomentLayout<DIM>::pa(k), b = MomentLayout<DIM>::pb(k);
+                            mw[k] = mc[k] + uw[a] * uw[b] - mc[1 + a] * mc[1 + b];
+                        }
+                        Coef<DIM> wc;
+                        wc.make(mw);
+                        const float fout = wc.population(cx, cy, cz);
+                        float fin = own.population(-cx, -cy, -cz);
+                        if (HALF) fin = round_half(fin);
+                        fin = fmaxf(fin, 0.0f);
+                        pop = fout;
+                        done = true;
+                        // momentum exchange, lattice units: fin (-c - uw) - fout (c - uw)
+                        const float c3[3] = {(float)cx, (float)cy, (float)cz};
+                        float F[3];
+#pragma unroll
+                        for (int k = 0; k < DIM; ++k) F[k] = fin * (-c3[k] - uw[k]) - fout * (c3[k] - uw[k]);
+                        has_share = true;
+                        hit_elem = e;
+#pragma unroll
+                        for (int j = 0; j < DIM; ++j) {
+                            vshare[j] = vv[j];
+#pragma unroll
+                            for (int k = 0; k < DIM; ++k) share[j][k] = F[k] * h.b[j];
+                        }
+                    }
+                }
+            }
+            if (!done) {
+                // ordinary pull from the (clamped or wrapped) upstream cell
+                const int sx = halo_index(x1, g.nx, wx), sy = halo_index(y1, g.ny, wy), sz = halo_index(z1, g.nz, wz);
+                const uint32_t sidx = (uint32_t)((long long)sz * nxy + (long long)sy * g.nx + sx);
+                float mn[NM];
+                load_moments<DIM, T>(mn, g.src, g.ncell, sidx, g.codec);
+                Coef<DIM> nc;
+                nc.make(mn);
+                float v = nc.population(cx, cy, cz);
+                if (HALF) v = round_half(v);
+                pop = fmaxf(v, 0.0f);
+            }
+        }
+        // forces: one share per (link, element vertex), summed per element
+        add_forces_warp<DIM>(acc, has_share, hit_elem, vshare, share, g.status);
+        // raw moments by warp reduction
+        int cx = 0, cy = 0, cz = 0;
+        if (lane < Q) dir_vec<DIM>(lane, cx, cy, cz);
+        const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
+        float R[NM];
+        if (DIM == 2) {
+            R[0] = pop; R[1] = pop * fx; R[2] = pop * fy;
+            R[3] = pop * fx * fx; R[4] = pop * fy * fy; R[5] = pop * fx * fy;
+        } else {
+            R[0] = pop; R[1] = pop * fx; R[2] = pop * fy; R[3] = pop * fz;
+            R[4] = pop * fx * fx; R[5] = pop * fy * fy; R[6] = pop * fz * fz;
+            R[7] = pop * fx * fy; R[8] = pop * fy * fz; R[9] = pop * fx * fz;
+        }
+#pragma unroll
+        for (int k = 0; k < NM; ++k)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) R[k] += __shfl_xor_sync(full, R[k], o);
+        if (lane == 0) {
+            float m[NM];
+            if (DIM == 2) collide2(R, g.omega, m);
+            else collide3(R, g.omega, m);
+            T *planes[NM];
+#pragma unroll
+            for (int k = 0; k < NM; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
+            encode_store<DIM, T>(m, planes, cell, g.codec);
+            if (bad_state<DIM>(m)) atomicOr(g.status, kStatusNonFinite);
+            if (f8 & kBitOutletSrc) {
+                float ms[NM];
+                stored_values<DIM, T>(m, ms, g.codec);
+                feed_outlets<DIM, T>(g, cell, ms, g.wallmask[cell]);
+            }
+        }
+    }
+}
+
+} // namespace fflbm

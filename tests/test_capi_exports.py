@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports exactly what include/ffs_lbm.h declares (no GPU)."""
+"""The C-ABI library loads and exports every entry point include/*.h declares (no GPU)."""
 import ctypes
 import os
 import re
@@ -10,9 +10,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_entry_points():
-    src = open(os.path.join(ROOT, "include", "ffs_lbm.h")).read()
-    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(ffs_\w+)\s*\(", src)))
+    names = set()
+    for h in ("ffs_lbm.h", "ffs_pool.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names |= set(re.findall(r"\b(ffs_\w+)\s*\(", src))
+    return sorted(names)
 
 
 def test_library_builds_and_loads():

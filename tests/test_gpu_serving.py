@@ -1,0 +1,192 @@
+"""The batched serving pool on the GPU, through the C ABI (include/ffs_pool.h).
+
+  * pool (FP32 storage) vs one grid per episode through ffs_lbm_step, fed the
+    same surface: moments and last-substep forces identical (the batched
+    kernels run the single-grid bodies on the same inputs)
+  * pool vs the ref32 oracle: moments max |diff| <= 2e-6, forces <= 1e-4 x max |F|
+  * an episode alone and in a mix of other episodes: every output identical
+  * FP16 storage vs the FP64 oracle: relative L2 velocity error <= 1e-3
+    (closed tank; FP32 storage, for scale, <= 5e-4)
+  * admission by device memory, eviction, and graph reuse across mixes
+"""
+import numpy as np
+import pytest
+
+from freeflow_b200 import serving as S
+
+from helpers import max_abs
+
+pytestmark = pytest.mark.gpu
+
+
+def _actions(sp, step):
+    return np.random.default_rng(sp.seed * 1000 + step).uniform(-1, 1, 8).astype(np.float32)
+
+
+def _run_pool(pool, slots_specs, control_steps):
+    """Advances the pool; returns per slot the output records and forces of every control step."""
+    outs = {s: [] for s, _ in slots_specs}
+    for c in range(control_steps):
+        for s, sp in slots_specs:
+            pool.set_action(s, _actions(sp, c))
+        pool.advance()
+        for s, sp in slots_specs:
+            o, F = pool.collect(s, forces=True)
+            outs[s].append((o.energy, o.force[0], o.force[1], o.torque, o.status, F))
+    return outs
+
+
+def test_pool_f32_matches_single_grid_step(cuda):
+    specs = [S.make_episode(256, 128, seed=11, length=10), S.make_episode(512, 192, seed=12, length=10)]
+    pool = S.Pool(storage="f32", budget_bytes=1 << 30, max_episodes=8)
+    slots = [(pool.admit(sp), sp) for sp in specs]
+    outs = _run_pool(pool, slots, 3)
+    for (s, sp) in slots:
+        env = S.PlainEnv(sp)
+        for c in range(3):
+            env.set_action(_actions(sp, c))
+            F = env.control_step(pool.substeps)
+        assert np.array_equal(pool.get_moments(s), env.g.get_moments()), "moments differ from ffs_lbm_step"
+        assert np.array_equal(outs[s][-1][5], F), "forces differ from ffs_lbm_step"
+        assert np.abs(F).max() > 0
+        env.close()
+    pool.close()
+
+
+def test_pool_matches_oracle(cuda):
+    from oracle.oracle import Oracle
+
+    sp = S.make_episode(256, 128, seed=21, length=10)
+    pool = S.Pool(storage="f32", budget_bytes=256 << 20, max_episodes=2)
+    s = pool.admit(sp)
+    o = Oracle(2, sp.nx, sp.ny, 1, viscosity=sp.viscosity, density=sp.density, dx=sp.dx, dt=sp.dt,
+               boundary_velocities=[0, 0, 0, 0], periodic=0, precision="ref32")
+    o.set_flags(sp.flags)
+    o.set_moments(pool.get_moments(s).astype(np.float64))
+    F = np.zeros(sp.rest.size)
+    q = 0
+    for c in range(2):
+        a = _actions(sp, c)
+        pool.set_action(s, a)
+        pool.advance()
+        for j in range(pool.substeps):
+            V, U = S.swimmer_surface(sp, a, q)
+            if j == pool.substeps - 1:
+                F[:] = 0.0
+            o.step(V, U, sp.elements, F)
+            q += 1
+    _, Fg = pool.collect(s, forces=True)
+    assert max_abs(pool.get_moments(s), o.get_moments()) <= 2e-6
+    assert max_abs(Fg.reshape(-1), F) <= 1e-4 * np.abs(F).max()
+    o.close()
+    pool.close()
+
+
+def test_episode_alone_and_in_mix_identical(cuda):
+    target = S.make_episode(512, 192, seed=31, length=10)
+    others = [S.make_episode(n[0], n[1], seed=40 + i, length=10)
+              for i, n in enumerate([(256, 128), (1200, 400), (512, 192), (256, 128), (1200, 400)])]
+    alone = S.Pool(storage="f16", budget_bytes=1 << 30, max_episodes=8)
+    sa = alone.admit(target)
+    out_a = _run_pool(alone, [(sa, target)], 4)[sa]
+    m_a = alone.get_moments(sa)
+    alone.close()
+
+    mix = S.Pool(storage="f16", budget_bytes=1 << 30, max_episodes=8)
+    pairs = [(mix.admit(sp), sp) for sp in others[:3]]
+    sm = mix.admit(target)                       # a different slot and table position
+    pairs += [(sm, target)] + [(mix.admit(sp), sp) for sp in others[3:]]
+    assert sm != sa
+    out_m = _run_pool(mix, pairs, 4)[sm]
+    m_m = mix.get_moments(sm)
+    mix.close()
+    for a, m in zip(out_a, out_m):
+        assert a[:5] == m[:5]
+        assert np.array_equal(a[5], m[5])
+    assert np.array_equal(m_a, m_m)
+
+
+@pytest.mark.parametrize("storage,tol", [("f16", 1e-3), ("f32", 5e-4)])
+def test_reduced_storage_velocity_error_vs_fp64(cuda, storage, tol):
+    """Relative L2 velocity error of the pool's state against the FP64 oracle,
+    fed the same surfaces, after 20 control steps (200 substeps) of a 256x128
+    swimmer in a closed tank.
+
+    The tank has walls because the reference's outlet rule switches on the
+    sign of the neighbour's normal velocity: where that velocity is near zero,
+    any two precisions, FP32 against FP64 included, take different branches.
+    With outlets, the FP32 oracle already differs from the FP64 one by 1.5e-4
+    relative after 200 substeps (the FP32 GPU path by 3e-3), whatever the
+    storage.  The closed tank isolates the storage error."""
+    from oracle.oracle import Oracle
+
+    sp = S.make_episode(256, 128, seed=51, length=50, sides="walls")
+    pool = S.Pool(storage=storage, budget_bytes=256 << 20, max_episodes=2)
+    s = pool.admit(sp)
+    o = Oracle(2, sp.nx, sp.ny, 1, viscosity=sp.viscosity, density=sp.density, dx=sp.dx, dt=sp.dt,
+               boundary_velocities=[0, 0, 0, 0], periodic=0, precision="phys64")
+    o.set_flags(sp.flags)
+    o.set_moments(pool.get_moments(s).astype(np.float64))
+    q = 0
+    for c in range(20):
+        a = _actions(sp, c)
+        pool.set_action(s, a)
+        pool.advance()
+        for _ in range(pool.substeps):
+            V, U = S.swimmer_surface(sp, a, q)
+            o.step(V, U, sp.elements, None)
+            q += 1
+    out, _ = pool.collect(s)
+    assert out.status == 0
+    g, ref = pool.get_moments(s).astype(np.float64), o.get_moments()
+    du = g[:, 1:3] - ref[:, 1:3]
+    rel = np.linalg.norm(du) / np.linalg.norm(ref[:, 1:3])
+    assert np.linalg.norm(ref[:, 1:3]) > 0
+    assert rel <= tol, f"{storage}: relative velocity error {rel:.3e}"
+    o.close()
+    pool.close()
+
+
+def test_admission_by_memory_and_eviction(cuda):
+    big = S.make_episode(1200, 400, seed=61, length=10)
+    small = S.make_episode(256, 128, seed=62, length=10)
+    probe = S.Pool(storage="f16", budget_bytes=64 << 20, max_episodes=4)
+    nb = probe.episode_bytes(big)
+    probe.close()
+    pool = S.Pool(storage="f16", budget_bytes=2 * nb + nb // 2, max_episodes=8)
+    a = pool.admit(big)
+    b = pool.admit(big)
+    assert a is not None and b is not None
+    assert pool.admit(big) is None               # over budget: refused, nothing changed
+    assert pool.info()["active_episodes"] == 2
+    c = pool.admit(small)                        # a smaller episode still fits
+    assert c is not None
+    pool.set_action(a, np.zeros(8, np.float32))
+    pool.advance()
+    pool.evict(a)
+    d = pool.admit(big)                          # memory freed by the eviction
+    assert d is not None
+    pool.advance()
+    for s in (b, c, d):
+        o, _ = pool.collect(s)
+        assert o.status == 0
+    pool.close()
+
+
+def test_graph_reused_across_mixes(cuda):
+    specs = [S.make_episode(512, 192, seed=70 + i, length=10) for i in range(6)]
+    pool = S.Pool(storage="f16", budget_bytes=1 << 30, max_episodes=8)
+    slots = [pool.admit(sp) for sp in specs[:4]]
+    pool.advance()
+    builds = pool.info()["graph_builds"]
+    pool.evict(slots[0])
+    slots.append(pool.admit(specs[4]))
+    pool.advance()
+    pool.evict(slots[1])
+    slots.append(pool.admit(specs[5]))
+    pool.advance()
+    info = pool.info()
+    assert info["graph_builds"] == builds        # the mix changed, the graph did not
+    assert info["advances"] == 3
+    assert info["active_episodes"] == 4
+    pool.close()
