@@ -1,0 +1,75 @@
+"""Every D3Q27 dense-kernel variant against the oracle (the tuner picks one
+per grid by speed, so each must pass the parity cases on its own).
+
+Variants: 0 and 1 are the single-plane z-march built for two and three CTAs
+per SM; 2 is the pair kernel (two planes per step in f32x2, FP32 storage).
+Tolerances are those of test_gpu_parity.py: 2e-6 against the ref32 oracle,
+4e-6 next to walls (bounce-back added as a correction), 5e-6 against FP64.
+"""
+import numpy as np
+import pytest
+
+from freeflow_b200 import workloads as W
+
+from helpers import max_abs, run_pair
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [0, 1, 2]
+
+
+@pytest.fixture(params=VARIANTS)
+def variant(request, monkeypatch):
+    monkeypatch.setenv("FFS_DENSE3D_VARIANT", str(request.param))
+    return request.param
+
+
+def test_swimmer(cuda, variant):
+    wl = W.swimmer_3d(nx=64, ny=32, nz=32, body_frac=0.3, nlat=12, nlon=16, seed=5)
+    gm, om, gf, of, st = run_pair(wl, 6)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+    assert max_abs(gf, of) <= 1e-4 * np.abs(of).max()
+
+
+def test_taylor_green_periodic_vs_fp64(cuda, variant):
+    wl = W.taylor_green_3d(n=32, u0=0.04, viscosity=0.005)
+    gm, om, _, _, st = run_pair(wl, 20, precision="phys64")
+    assert st == 0
+    assert max_abs(gm, om) <= 5e-6
+
+
+def test_clamped_halo(cuda, variant):
+    wl = W.taylor_green_3d(n=20, u0=0.04, viscosity=0.01)
+    gm, om, _, _, st = run_pair(wl, 8, periodic=0)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+
+
+def test_walls_inlet_outlet(cuda, variant):
+    wl = W.swimmer_3d(nx=40, ny=24, nz=24, nlat=8, nlon=12)
+    wl.elements = None
+    gm, om, _, _, st = run_pair(wl, 8)
+    assert st == 0
+    assert max_abs(gm, om) <= 4e-6
+
+
+def test_open_face_with_wall_across_the_wrap(cuda, variant):
+    wl = W.taylor_green_3d(n=20, u0=0.03, viscosity=0.01)
+    f = wl.flags.reshape(20, 20, 20)
+    f[:, :, 19] = W.WALL
+    f[0, :, :] = W.WALL
+    wl.flags = f.reshape(-1)
+    gm, om, _, _, st = run_pair(wl, 6, periodic=0)
+    assert st == 0
+    assert max_abs(gm, om) <= 4e-6
+
+
+@pytest.mark.parametrize("nz", [17, 40])
+def test_odd_and_chunked_depths(cuda, variant, nz):
+    """Plane counts that leave a single plane in the last pair, and depths
+    split into several z chunks."""
+    wl = W.swimmer_3d(nx=48, ny=24, nz=nz, body_frac=0.3, nlat=8, nlon=12, seed=9)
+    gm, om, _, _, st = run_pair(wl, 4)
+    assert st == 0
+    assert max_abs(gm, om) <= 4e-6
