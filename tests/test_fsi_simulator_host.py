@@ -1,0 +1,135 @@
+"""The fsi_simulator mirror on the host (no GPU): JSON configuration with the
+reference's fields and defaults, node flags from the boundary list, Medit mesh
+reading, surface extraction and solid placement."""
+import json
+import math
+
+import numpy as np
+import pytest
+
+from freeflow_b200 import fsi_simulator as F
+from freeflow_b200 import meshio
+
+
+def _write(tmp_path, name, obj):
+    p = tmp_path / name
+    p.write_text(json.dumps(obj))
+    return str(p)
+
+
+def test_config2d_fields_defaults_and_boundaries(tmp_path):
+    path = _write(tmp_path, "c.json", {
+        "fluid_nx": 16, "fluid_ny": 8, "fluid_viscosity": 0.02, "dt": 0.0025, "fluid_dx": 0.005,
+        "boundary_velocities": [0.05, 0, 0, 0],
+        "boundaries": [{"pos": [0, 3], "type": "InletLeft"}, {"pos": [15, 3], "type": "OutletRight"},
+                       {"pos": [4, 0], "type": "Wall"}, {"pos": [4, 0], "type": "Bogus"}],
+        "solids": [{"mesh_path": "fish.mesh", "translate": [1, 2], "rotate": 30, "density": 50}],
+        "global_fem_options": {"iterations": 4},
+    })
+    c = F.Config2D()
+    with pytest.warns(UserWarning, match="unrecognized"):
+        assert c.load(path)
+    p = c.get_params()
+    assert (p.fluid_nx, p.fluid_ny, p.fluid_viscosity, p.dt, p.fluid_dx) == (16, 8, 0.02, 0.0025, 0.005)
+    assert p.fluid_density == 1000.0 and p.solid_solver_type == "static" and p.output_frequency == 100
+    assert p.boundary_velocities == [0.05, 0.0, 0.0, 0.0]
+    assert [b.flag for b in p.boundaries] == [13, 20, 5, 0]
+    s = p.solids[0]
+    assert s.mesh_path == "fish.mesh" and s.translate == [1.0, 2.0] and s.rotate == 30.0 and s.density == 50.0
+    assert s.scale == [1.0, 1.0] and s.lbs_control_config.cnum == 2
+    assert p.global_fem_options.iterations == 4 and p.global_fem_options.omega == 0.8
+    # getCf in float: rho dx^2 dx / dt^2
+    assert p.get_cf() == float(np.float32(float(np.float32(1000.0 * 0.005 * 0.005)) * 0.005 / 0.0025 ** 2))
+
+
+def test_config_defaults_when_fields_are_absent(tmp_path):
+    c2, c3 = F.Config2D(), F.Config3D()
+    assert c2.load(_write(tmp_path, "a.json", {}))
+    assert c3.load(_write(tmp_path, "b.json", {"fluid_nz": 12}))
+    p2, p3 = c2.get_params(), c3.get_params()
+    assert (p2.fluid_nx, p2.fluid_ny, p2.boundary_velocities) == (400, 400, [0.0] * 4)
+    assert (p3.fluid_nx, p3.fluid_ny, p3.fluid_nz, p3.boundary_velocities) == (128, 128, 12, [])
+
+
+def test_config_load_failures(tmp_path, capsys):
+    c = F.Config2D()
+    assert not c.load(str(tmp_path / "missing.json"))
+    bad = tmp_path / "bad.json"
+    bad.write_text("{ not json")
+    assert not c.load(str(bad))
+    assert not c.load(_write(tmp_path, "t.json", {"boundaries": [{"type": "Wall"}]}))  # no "pos"
+    assert "FATAL" in capsys.readouterr().err
+
+
+def test_flags_from_boundaries_later_entry_wins_and_outside_is_ignored():
+    p = F.SimulationParameters2D(fluid_nx=5, fluid_ny=4)
+    p.boundaries = [F.BoundaryCondition([0, 0], 5), F.BoundaryCondition([0, 0], 13),
+                    F.BoundaryCondition([4, 3], 20), F.BoundaryCondition([5, 0], 5)]
+    with pytest.warns(UserWarning, match="outside"):
+        f = F.flags_from_params(p)
+    assert f.shape == (20,) and f[0] == 13 and f[19] == 20 and (f[1:19] == F.FLUID).all()
+    p3 = F.SimulationParameters3D(fluid_nx=3, fluid_ny=2, fluid_nz=2)
+    p3.boundaries = [F.BoundaryCondition([2, 1, 1], 24)]
+    f3 = F.flags_from_params(p3)
+    assert f3[(1 * 2 + 1) * 3 + 2] == 24 and (f3 == F.FLUID).sum() == 11
+
+
+def _square_mesh(n):
+    xs = np.linspace(0.0, 1.0, n + 1)
+    v = np.array([[x, y] for y in xs for x in xs])
+    t = []
+    for j in range(n):
+        for i in range(n):
+            a = j * (n + 1) + i
+            t += [[a, a + 1, a + n + 2], [a, a + n + 2, a + n + 1]]
+    return v, np.array(t)
+
+
+def test_medit_round_trip_and_2d_surface(tmp_path):
+    v, t = _square_mesh(4)
+    path = str(tmp_path / "sq.mesh")
+    meshio.write_medit(path, v, triangles=t)
+    m = meshio.load_medit(path, dimension=2)
+    assert np.allclose(m.vertices, v) and np.array_equal(m.triangles, t)
+    sv, se, ids = meshio.surface_of(m)
+    assert se.shape == (16, 2) and len(sv) == 16          # 4 x 4 boundary edges, 16 boundary vertices
+    # every boundary vertex lies on the unit square's boundary
+    on = np.isclose(sv[:, 0], 0) | np.isclose(sv[:, 0], 1) | np.isclose(sv[:, 1], 0) | np.isclose(sv[:, 1], 1)
+    assert on.all()
+    # oriented edges form closed loops: every vertex starts exactly one edge and ends exactly one
+    assert np.array_equal(np.sort(se[:, 0]), np.arange(16)) and np.array_equal(np.sort(se[:, 1]), np.arange(16))
+
+
+def test_tet_boundary_faces():
+    # a cube split into 6 tetrahedra around the diagonal 0-6: 12 boundary triangles
+    v = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    tets = np.array([[0, 1, 2, 6], [0, 2, 3, 6], [0, 3, 7, 6], [0, 7, 4, 6], [0, 4, 5, 6], [0, 5, 1, 6]])
+    faces = meshio.boundary_faces(tets)
+    assert faces.shape == (12, 3)
+    sv, se, _ = meshio.surface_of(meshio.MeditMesh(3, v, np.zeros((0, 3), int), tets))
+    assert len(sv) == 8 and se.shape == (12, 3)
+
+
+def test_medit_rejects_wrong_dimension_and_short_entries(tmp_path):
+    v, t = _square_mesh(1)
+    path = str(tmp_path / "s.mesh")
+    meshio.write_medit(path, v, triangles=t)
+    with pytest.raises(ValueError, match="3D mesh was expected"):
+        meshio.load_medit(path, dimension=3)
+    bad = tmp_path / "b.mesh"
+    bad.write_text("MeshVersionFormatted 1\nDimension 2\nVertices\n2\n0 0\n1\n")
+    with pytest.raises(ValueError, match="short"):
+        meshio.load_medit(str(bad))
+
+
+def test_place_follows_the_reference_conventions():
+    # 2D: scale, then the reference's rotation (points turn by -rotate), then translate
+    p = meshio.place(np.array([[1.0, 0.0]]), [10.0, 20.0], 90.0, [2.0, 1.0])
+    assert np.allclose(p, [[10.0, 18.0]])
+    # 3D: R = Ry(rot[1]) Rx(rot[0]) Rz(rot[2]); a quarter turn about z maps x to y
+    q = meshio.place(np.array([[1.0, 0.0, 0.0]]), [0, 0, 0], [0.0, 0.0, 90.0], [1, 1, 1])
+    assert np.allclose(q, [[0.0, 1.0, 0.0]], atol=1e-12)
+    r = meshio.place(np.array([[0.0, 0.0, 1.0]]), [0, 0, 0], [0.0, 90.0, 0.0], [1, 1, 1])
+    assert np.allclose(r, [[1.0, 0.0, 0.0]], atol=1e-12)
+    assert math.isclose(np.linalg.norm(meshio.place(np.array([[3.0, 4.0, 0.0]]), [0, 0, 0], [10, 20, 30],
+                                                    [1, 1, 1])), 5.0)
