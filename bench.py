@@ -221,8 +221,10 @@ def oracle_slab_run(wl: W.Workload, steps: int, warmup: int, nz_slab: int, threa
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    from freeflow_b200 import replicas as R
+
+    rank, _, _ = R.env_ranks()
+    if rank != 0:  # the CPU reference arm runs once, on rank 0; other ranks exit without work
         return 0
     wl = make_workload(args.workload, args.small)
     threads = os.cpu_count() or 1
@@ -354,17 +356,12 @@ def run_serving_line(args):
 # ------------------------------------------------------------------- GPU
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
+    from freeflow_b200 import replicas as R
+
+    rank, world, local = R.env_ranks()
+    torch.cuda.set_device(local if world > 1 else 0)
+    R.init("nccl", timeout_s=300.0, device=torch.device("cuda", local) if world > 1 else None)
     from freeflow_b200 import DeviceSurface, FluidGrid
 
     wl = make_workload(args.workload, args.small)
@@ -408,8 +405,7 @@ def run_ours(args):
 
     # ---- timed region: inputs resident in HBM (both moment buffers exceed L2)
     clocks = ClockSampler(torch.cuda.current_device())
-    if world > 1:
-        dist.barrier()
+    R.barrier()
     torch.cuda.synchronize()
     g.profile(True)
     g.profile_read(reset=True)
@@ -424,12 +420,8 @@ def run_ours(args):
     clk = clocks.stop()
     g.profile(False)
     prof = g.profile_read(reset=True)
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = R.max_over_ranks(ev0.elapsed_time(ev1), device="cuda")
+    R.barrier()
     status = g.status(clear=True)
 
     # ---- end to end: host surface in pinned memory -> step -> forces to host
@@ -453,8 +445,7 @@ def run_ours(args):
             for s in range(Wm):
                 e2e_step(s)
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        R.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         with torch.cuda.stream(stream):
@@ -462,20 +453,16 @@ def run_ours(args):
                 e2e_step(Wm + s)
         e1.record(stream)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = R.max_over_ranks(e0.elapsed_time(e1), device="cuda")
         nb = surf.num_vertices * wl.dim * 4
-        e2e = {"value": round(world * wl.ncell * K / (ems * 1e-3) / 1e6, 1), "unit": "MLUPS",
+        e2e = {"value": round(R.whole_job_rate(wl.ncell * K, ems * 1e-3, world) / 1e6, 1), "unit": "MLUPS",
                "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb}
     else:
         # no surface: the step's inputs are the moments themselves; e2e = upload
         # the initial state once, step, read back the density field once
         e2e = None
 
-    value = world * wl.ncell * K / (ms * 1e-3) / 1e6
+    value = R.whole_job_rate(wl.ncell * K, ms * 1e-3, world) / 1e6
     peak, peak_kind = hbm_peak()
     bpc = algorithmic_bytes_per_cell(wl.dim, storage)
     dense_ms, dense_n = prof["dense"]
@@ -521,9 +508,7 @@ def run_ours(args):
             out["serving"] = run_serving(iterations=150, warmup=20)
         print(json.dumps(out), flush=True)
     g.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.shutdown()
     return 0
 
 

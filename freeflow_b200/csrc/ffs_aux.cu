@@ -112,33 +112,73 @@ cudaError_t launch_initialize(const GridArgs<T> &g, T *other, const float *bcvel
     return cudaGetLastError();
 }
 
-// updateSolidFlagKernel / resetSolidFlagKernel with the even-odd crossing
-// test of SolidGeometryProxy_Device<2>::isInside (:126-144), each operation
-// explicitly rounded so the mask matches the CPU oracle exactly.
-__global__ void fill_solid2_kernel(uint8_t *flags, int nx, int ny, float cl, SurfaceArgs s)
+// fillSolidFlags2D (FsiCoupling2D.cu:318-354, 434-464): a Fluid or
+// SolidDynamic cell becomes SolidDynamic when its centre is inside the closed
+// polygon, Fluid otherwise.  The reference tests every cell against every edge
+// (crossing-number parity, SolidGeometryProxy_Device.cuh:126-144).  Here one
+// warp takes one row: the crossing abscissae of the row's scanline with the
+// edges are computed once per row, with the same explicitly rounded
+// operations as the reference's per-cell expression, and each cell's parity
+// is the number of crossings to its right.  Every operation is explicitly
+// rounded, so the mask is bit-identical to the per-cell test (and to the CPU
+// oracle); a row with more crossings than fit in shared memory falls back to
+// the per-cell test.
+constexpr int kFillCrossings = 256;
+
+__global__ void __launch_bounds__(256) fill_solid2_kernel(uint8_t *flags, int nx, int ny, float cl, SurfaceArgs s)
 {
     using namespace geom;
-    const long long n = (long long)nx * ny;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        uint32_t t = flags[c] & kTypeMask;
-        if (t != kFluid && t != kSolidDynamic) continue;
-        const int x = (int)(c % nx), y = (int)(c / nx);
-        const float px = mul(add((float)x, 0.5f), cl), py = mul(add((float)y, 0.5f), cl);
-        bool in = false;
-        for (int i = 0; i < s.ne; ++i) {
-            uint32_t a = s.E[2 * i], b = s.E[2 * i + 1];
-            float sx = s.V[2 * a], sy = s.V[2 * a + 1], tx = s.V[2 * b], ty = s.V[2 * b + 1];
-            if ((sy < py && ty >= py) || (sy >= py && ty < py))
-                in ^= (add(sx, dvd(mul(sub(py, sy), sub(tx, sx)), sub(ty, sy))) > px);
+    __shared__ float xs_all[8][kFillCrossings];
+    float *xs = xs_all[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int y = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); y < ny; y += nwarps) {
+        const float py = mul(add((float)y, 0.5f), cl);
+        int count = 0;
+        for (int i0 = 0; i0 < s.ne; i0 += 32) {
+            const int i = i0 + lane;
+            bool cross = false;
+            float xc = 0.0f;
+            if (i < s.ne) {
+                const uint32_t a = s.E[2 * i], b = s.E[2 * i + 1];
+                const float sx = s.V[2 * a], sy = s.V[2 * a + 1], tx = s.V[2 * b], ty = s.V[2 * b + 1];
+                if ((sy < py && ty >= py) || (sy >= py && ty < py)) {
+                    cross = true;
+                    xc = add(sx, dvd(mul(sub(py, sy), sub(tx, sx)), sub(ty, sy)));
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, cross);
+            const int pos = count + __popc(m & below);
+            if (cross && pos < kFillCrossings) xs[pos] = xc;
+            count += __popc(m);
         }
-        flags[c] = in ? kSolidDynamic : kFluid;
+        __syncwarp();
+        for (int x = lane; x < nx; x += 32) {
+            const size_t c = (size_t)y * nx + x;
+            const uint32_t t = flags[c] & kTypeMask;
+            if (t != kFluid && t != kSolidDynamic) continue;
+            const float px = mul(add((float)x, 0.5f), cl);
+            bool in = false;
+            if (count <= kFillCrossings) {
+                for (int k = 0; k < count; ++k) in ^= (xs[k] > px);
+            } else {
+                for (int i = 0; i < s.ne; ++i) {
+                    const uint32_t a = s.E[2 * i], b = s.E[2 * i + 1];
+                    const float sx = s.V[2 * a], sy = s.V[2 * a + 1], tx = s.V[2 * b], ty = s.V[2 * b + 1];
+                    if ((sy < py && ty >= py) || (sy >= py && ty < py))
+                        in ^= (add(sx, dvd(mul(sub(py, sy), sub(tx, sx)), sub(ty, sy))) > px);
+                }
+            }
+            flags[c] = in ? kSolidDynamic : kFluid;
+        }
+        __syncwarp();
     }
 }
 
 cudaError_t launch_fill_solid2(uint8_t *flags, int nx, int ny, float cl, const SurfaceArgs &s, cudaStream_t st)
 {
-    long long n = (long long)nx * ny;
-    int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    const int grid = std::max(1, std::min((ny + 7) / 8, 148 * 8));
     fill_solid2_kernel<<<grid, 256, 0, st>>>(flags, nx, ny, cl, s);
     return cudaGetLastError();
 }

@@ -113,6 +113,9 @@ __global__ void pool_detect_kernel(const PoolEpisode *eps, const PoolActive *act
 }
 
 // ----------------------------------------------------------------- dense
+// Persistent CTAs stride over the tiles of all episodes in order, so a CTA's
+// episode index only grows: it is advanced from the previous tile's instead of
+// searched.
 template <typename T, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
 {
@@ -120,12 +123,13 @@ __global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *
     const int n = (int)act->n;
     if (n == 0) return;
     const uint32_t total = act->tile_prefix[n];
+    int a = 0;
     for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
-        const int a = owner_of(act->tile_prefix, n, t);
+        while (act->tile_prefix[a + 1] <= t) ++a;
         const uint32_t local = t - act->tile_prefix[a];
-        const uint32_t tx = local % act->tiles_x[a], ty = local / act->tiles_x[a];
+        const uint32_t tw = act->tiles_x[a];
         const GridArgs<T> g = episode_args<T>(eps[act->slot[a]], parity);
-        dense2d_tile<T, false, TX, TY>(g, (int)tx * TX, (int)ty * TY, sp);
+        dense2d_tile<T, false, TX, TY>(g, (int)(local % tw) * TX, (int)(local / tw) * TY, sp);
         __syncthreads(); // the next tile reuses sp
     }
 }

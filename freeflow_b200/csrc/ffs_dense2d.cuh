@@ -24,31 +24,67 @@ __device__ __forceinline__ int halo_index(int v, int n, bool wrap)
     return v;
 }
 
-// Processes the TX x TY tile with lower-left cell (x0, y0).  The caller's
-// CTA has TX * TY threads; sp is the CTA's population tile (tile + halo).
-template <typename T, bool HALF, int TX = D2::kTX, int TY = D2::kTY>
-__device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y0, float (*sp)[TY + 2][TX + 2])
+// Halo cells of a TX x TY tile per thread (at most two for every shape used).
+template <int TX, int TY> struct Halo2 {
+    static constexpr int kHX = TX + 2, kHalo = (TX + 2) * (TY + 2), kThreads = TX * TY;
+    static constexpr int kPer = (kHalo + kThreads - 1) / kThreads;
+};
+
+// Stored moments of the thread's halo cells of the tile at (x0, y0), as they
+// are in memory (step 1 of dense2d_tile decodes them).  Issued ahead of use,
+// these loads overlap the previous tile's work.
+template <typename T, int TX, int TY>
+__device__ __forceinline__ void dense2d_load(const GridArgs<T> &g, int x0, int y0, T (&raw)[Halo2<TX, TY>::kPer][6])
+{
+    using H = Halo2<TX, TY>;
+    const bool wx = g.periodic & 1, wy = g.periodic & 2;
+#pragma unroll
+    for (int r = 0; r < H::kPer; ++r) {
+        const int c = threadIdx.x + r * H::kThreads;
+        if (c < H::kHalo) {
+            const int hx = c % H::kHX, hy = c / H::kHX;
+            const int gx = halo_index(x0 + hx - 1, g.nx, wx);
+            const int gy = halo_index(y0 + hy - 1, g.ny, wy);
+            const uint32_t idx = (uint32_t)(gy * g.nx + gx);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) raw[r][k] = g.src[(size_t)k * g.ncell + idx];
+        }
+    }
+}
+
+// Processes the TX x TY tile with lower-left cell (x0, y0) from the halo
+// moments `raw` (dense2d_load).  The caller's CTA has TX * TY threads; sp is
+// the CTA's population tile (tile + halo).  after_recon() runs once the halo
+// is reconstructed and raw is no longer needed (a persistent caller loads its
+// next tile there).
+template <typename T, bool HALF, int TX, int TY, typename After>
+__device__ __forceinline__ void dense2d_tile_loaded(const GridArgs<T> &g, int x0, int y0, float (*sp)[TY + 2][TX + 2],
+                                                    const T (&raw)[Halo2<TX, TY>::kPer][6], After &&after_recon)
 {
     using L = Lattice<2>;
-    constexpr int kHX = TX + 2, kHalo = (TX + 2) * (TY + 2), kThreads = TX * TY;
+    using H = Halo2<TX, TY>;
     const int tid = threadIdx.x;
-    const bool wx = g.periodic & 1, wy = g.periodic & 2;
 
     // 1. reconstruct the tile + halo.  The halo index is clamped (the
     //    reference's min/max, FsiCoupling2D.cu:104-105) or wrapped (periodic).
-    for (int c = tid; c < kHalo; c += kThreads) {
-        int hx = c % kHX, hy = c / kHX;
-        int gx = halo_index(x0 + hx - 1, g.nx, wx);
-        int gy = halo_index(y0 + hy - 1, g.ny, wy);
-        float m[6];
-        load_moments<2, T>(m, g.src, g.ncell, (uint32_t)(gy * g.nx + gx), g.codec);
-        Coef<2> cf;
-        cf.make(m);
-        float f[9];
-        cf.populations(f);
 #pragma unroll
-        for (int i = 0; i < 9; ++i) sp[i][hy][hx] = HALF ? round_half(f[i]) : f[i];
+    for (int r = 0; r < H::kPer; ++r) {
+        const int c = tid + r * H::kThreads;
+        if (c < H::kHalo) {
+            const int hx = c % H::kHX, hy = c / H::kHX;
+            float m[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) m[k] = StorageTraits<T>::from(raw[r][k]);
+            decode_moments<2, T>(m, g.codec);
+            Coef<2> cf;
+            cf.make(m);
+            float f[9];
+            cf.populations(f);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) sp[i][hy][hx] = HALF ? round_half(f[i]) : f[i];
+        }
     }
+    after_recon();
     __syncthreads();
 
     const int tx = tid % TX, ty = tid / TX;
@@ -84,6 +120,15 @@ __device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y
             }
         }
     }
+}
+
+// The tile with its own loads (the single-grid kernel).
+template <typename T, bool HALF, int TX = D2::kTX, int TY = D2::kTY>
+__device__ __forceinline__ void dense2d_tile(const GridArgs<T> &g, int x0, int y0, float (*sp)[TY + 2][TX + 2])
+{
+    T raw[Halo2<TX, TY>::kPer][6];
+    dense2d_load<T, TX, TY>(g, x0, y0, raw);
+    dense2d_tile_loaded<T, HALF, TX, TY>(g, x0, y0, sp, raw, [] {});
 }
 
 template <typename T> cudaError_t launch_dense2d(const GridArgs<T> &g, cudaStream_t s);
