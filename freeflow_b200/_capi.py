@@ -38,7 +38,8 @@ EXPORTS = (
     "ffs_lbm_profile_enable", "ffs_lbm_profile_read",
     "ffs_status_string", "ffs_last_error", "ffs_abi_version",
     "ffs_pool_create", "ffs_pool_destroy", "ffs_pool_episode_bytes", "ffs_pool_admit", "ffs_pool_evict",
-    "ffs_pool_set_action", "ffs_pool_advance", "ffs_pool_collect", "ffs_pool_get_moments", "ffs_pool_tune",
+    "ffs_pool_set_action", "ffs_pool_set_actions", "ffs_pool_advance", "ffs_pool_collect", "ffs_pool_collect_many",
+    "ffs_pool_get_moments", "ffs_pool_tune",
     "ffs_pool_get_info", "ffs_swimmer_surface",
 )
 
@@ -142,6 +143,8 @@ def load():
         "ffs_pool_admit": [vp, C.POINTER(EpisodeDesc), C.POINTER(i32)],
         "ffs_pool_evict": [vp, i32],
         "ffs_pool_set_action": [vp, i32, vp, i32],
+        "ffs_pool_set_actions": [vp, i32, vp, vp],
+        "ffs_pool_collect_many": [vp, i32, vp, vp],
         "ffs_pool_advance": [vp],
         "ffs_pool_collect": [vp, i32, C.POINTER(PoolOutput), vp],
         "ffs_pool_get_moments": [vp, i32, vp],

@@ -611,6 +611,18 @@ ffs_status ffs_pool_set_action(ffs_pool *p, int slot, const float *actions, int 
     return FFS_OK;
 }
 
+ffs_status ffs_pool_set_actions(ffs_pool *p, int n, const int *slots, const float *actions)
+{
+    if (!p || n < 0 || (n > 0 && (!slots || !actions))) return fail(FFS_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < n; ++i)
+        if (slots[i] < 0 || slots[i] >= (int)p->slots.size() || !p->slots[slots[i]].used)
+            return fail(FFS_ERR_INVALID_ARGUMENT, "no such episode: slot " + std::to_string(slots[i]));
+    const int na = p->d.num_actions;
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < na; ++k) p->slots[slots[i]].actions[k] = actions[(size_t)i * na + k];
+    return FFS_OK;
+}
+
 ffs_status ffs_pool_tune(ffs_pool *p)
 {
     if (!p) return fail(FFS_ERR_INVALID_ARGUMENT, "null pool");
@@ -672,6 +684,18 @@ ffs_status ffs_pool_collect(ffs_pool *p, int slot, ffs_pool_output *out, double 
         POOL_CK(cudaMemcpyAsync(forces, s.dev.force, sizeof(double) * 2 * s.nv, cudaMemcpyDeviceToHost, p->st));
         POOL_CK(cudaStreamSynchronize(p->st));
     }
+    return FFS_OK;
+}
+
+ffs_status ffs_pool_collect_many(ffs_pool *p, int n, const int *slots, ffs_pool_output *out)
+{
+    if (!p || n < 0 || (n > 0 && (!slots || !out))) return fail(FFS_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < n; ++i)
+        if (slots[i] < 0 || slots[i] >= (int)p->slots.size() || !p->slots[slots[i]].used)
+            return fail(FFS_ERR_INVALID_ARGUMENT, "no such episode: slot " + std::to_string(slots[i]));
+    ffs_status r = wait_idle(p);
+    if (r != FFS_OK) return r;
+    for (int i = 0; i < n; ++i) std::memcpy(out + i, p->h_out + slots[i], sizeof(ffs_pool_output));
     return FFS_OK;
 }
 

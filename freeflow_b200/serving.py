@@ -42,6 +42,10 @@ from . import workloads as W
 
 SERVING_SIZES = ((256, 128), (512, 192), (1200, 400))
 
+# ffs_pool_output as a numpy record (48 bytes)
+OUTPUT_DTYPE = np.dtype([("energy", "<f8"), ("force", "<f8", (2,)), ("torque", "<f8"), ("status", "<u4"),
+                         ("pad", "<u4")])
+
 
 def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data)
@@ -214,6 +218,19 @@ class Pool:
         a = np.ascontiguousarray(actions, dtype=np.float32)
         A.check(A.load().ffs_pool_set_action(self._h, int(slot), _ptr(a), int(a.size)), "ffs_pool_set_action")
 
+    def set_actions(self, slots, actions):
+        """Actions of many slots in one call: actions is (len(slots), num_actions)."""
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        a = np.ascontiguousarray(actions, dtype=np.float32).reshape(len(sl), self.num_actions)
+        A.check(A.load().ffs_pool_set_actions(self._h, int(sl.size), _ptr(sl), _ptr(a)), "ffs_pool_set_actions")
+
+    def collect_many(self, slots) -> np.ndarray:
+        """Output records of many slots (a structured array with the fields of ffs_pool_output)."""
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        out = np.zeros(sl.size, dtype=OUTPUT_DTYPE)
+        A.check(A.load().ffs_pool_collect_many(self._h, int(sl.size), _ptr(sl), _ptr(out)), "ffs_pool_collect_many")
+        return out
+
     def advance(self):
         A.check(A.load().ffs_pool_advance(self._h), "ffs_pool_advance")
 
@@ -337,14 +354,19 @@ def serve(pool: Pool, specs: list[EpisodeSpec], iterations: int, initial: int, a
             continue
         conc.append(len(live))
         pool.advance()
-        for slot in list(live):
-            out, _ = pool.collect(slot)
-            t = time.perf_counter()
+        slots = list(live)
+        if hasattr(pool, "collect_many"):
+            status = pool.collect_many(slots)["status"]
+        else:
+            status = [pool.collect(sl)[0].status for sl in slots]
+        t = time.perf_counter()
+        cont, acts = [], []
+        for slot, stat in zip(slots, status):
             st = live[slot]
             lat.append(t - st.submitted)
             steps += 1
             st.done_steps += 1
-            if out.status & A.STATUS_NONFINITE:
+            if int(stat) & A.STATUS_NONFINITE:
                 diverged += 1
                 pool.evict(slot)
                 del live[slot]
@@ -353,8 +375,17 @@ def serve(pool: Pool, specs: list[EpisodeSpec], iterations: int, initial: int, a
                 pool.evict(slot)
                 del live[slot]
             else:
-                pool.set_action(slot, st.rng.uniform(-1.0, 1.0, pool.num_actions).astype(np.float32))
-                st.submitted = time.perf_counter()
+                cont.append(slot)
+                acts.append(st.rng.uniform(-1.0, 1.0, pool.num_actions).astype(np.float32))
+        if cont:
+            if hasattr(pool, "set_actions"):
+                pool.set_actions(cont, np.stack(acts))
+            else:
+                for slot, a in zip(cont, acts):
+                    pool.set_action(slot, a)
+            now = time.perf_counter()
+            for slot in cont:
+                live[slot].submitted = now
     wall = time.perf_counter() - (t_begin if t_begin is not None else time.perf_counter())
     info = pool.info() if hasattr(pool, "info") else None
     for slot in list(live):

@@ -117,6 +117,10 @@ ffs_status ffs_pool_evict(ffs_pool *pool, int slot);
  * previous action is kept until replaced.  n <= num_actions. */
 ffs_status ffs_pool_set_action(ffs_pool *pool, int slot, const float *actions, int n);
 
+/* ffs_pool_set_action for n slots in one call: actions holds n rows of
+ * num_actions values.  Nothing changes if a slot is invalid. */
+ffs_status ffs_pool_set_actions(ffs_pool *pool, int n, const int *slots, const float *actions);
+
 /* Launches one control step of every admitted episode; returns without
  * waiting.  The first call after the mix changed re-uploads the tile table;
  * the first call (and ffs_pool_tune) builds the CUDA graph. */
@@ -126,6 +130,9 @@ ffs_status ffs_pool_advance(ffs_pool *pool);
  * forces (optional): the slot's per-vertex fluid forces of the last
  * substep, (nv, 2) doubles. */
 ffs_status ffs_pool_collect(ffs_pool *pool, int slot, ffs_pool_output *out, double *forces);
+
+/* ffs_pool_collect of n slots' output records in one call (waits once). */
+ffs_status ffs_pool_collect_many(ffs_pool *pool, int n, const int *slots, ffs_pool_output *out);
 
 /* Current moments of the slot in the reference AoS layout (nx*ny*6 floats,
  * host memory); synchronous.  For tests and inspection. */

@@ -207,3 +207,34 @@ def test_deterministic_repeat(cuda):
     b = run_pair(wl, 4)
     assert np.array_equal(a[0], b[0])
     assert np.array_equal(a[2], b[2])
+
+
+def test_surface_in_the_solids_full_vertex_arrays(cuda):
+    """The step reads the solid's own vertex arrays: boundary elements that
+    index a full mesh (interior vertices included) give the same flow and the
+    same boundary forces as a gathered surface, and zero force on interior
+    vertices, so no gather or scatter pass is needed around the step."""
+    from freeflow_b200 import DeviceSurface
+
+    wl = small_swimmer_2d()
+    v, u = wl.surface_at(5)
+    nb = v.shape[0]
+    rng = np.random.default_rng(0)
+    interior = rng.uniform(v.min(0), v.max(0), size=(57, 2)).astype(np.float32)
+    # full mesh: interior vertices first, then the boundary ones
+    V = np.concatenate([interior, v])
+    U = np.concatenate([np.zeros_like(interior), u])
+    E = wl.elements.astype(np.uint32) + 57
+    g1, s1 = make_gpu(wl)
+    g2, _ = make_gpu(wl)
+    s1.update(v, u)
+    s2 = DeviceSurface(V, U, E, with_forces64=True)
+    for _ in range(4):
+        g1.step(s1)
+        g2.step(s2)
+    assert np.array_equal(g1.get_moments(), g2.get_moments())
+    f1 = s1.forces64.cpu().numpy()
+    f2 = s2.forces64.cpu().numpy()
+    assert np.array_equal(f2[57:], f1) and np.abs(f1).max() > 0
+    assert not f2[:57].any()
+    assert nb == f1.shape[0]

@@ -190,3 +190,27 @@ def test_graph_reused_across_mixes(cuda):
     assert info["advances"] == 3
     assert info["active_episodes"] == 4
     pool.close()
+
+
+def test_batched_action_and_output_calls_match_per_slot_calls(cuda):
+    specs = [S.make_episode(256, 128, seed=80 + i, length=10) for i in range(3)]
+    a = S.Pool(storage="f16", budget_bytes=256 << 20, max_episodes=4)
+    b = S.Pool(storage="f16", budget_bytes=256 << 20, max_episodes=4)
+    sa = [a.admit(sp) for sp in specs]
+    sb = [b.admit(sp) for sp in specs]
+    for c in range(3):
+        acts = np.stack([_actions(sp, c) for sp in specs])
+        for s, act in zip(sa, acts):
+            a.set_action(s, act)
+        b.set_actions(sb, acts)
+        a.advance()
+        b.advance()
+        ra = [a.collect(s)[0] for s in sa]
+        rb = b.collect_many(sb)
+        for o, r in zip(ra, rb):
+            assert (o.energy, o.force[0], o.force[1], o.torque, o.status) == \
+                (r["energy"], r["force"][0], r["force"][1], r["torque"], r["status"])
+    with pytest.raises(Exception, match="no such episode"):
+        b.set_actions([sb[0], 3], np.zeros((2, 8), np.float32))
+    a.close()
+    b.close()
