@@ -2,9 +2,10 @@
 // memory, and the per-step launch sequence.
 //
 // Per step, on the caller's stream and without host synchronisation:
-//   1. detect_links   (only with a surface)   O(surface)
+//   1. detect_links   (only with a surface)   O(surface), on a side stream,
+//                                             concurrent with 2
 //   2. dense2d/dense3d                         O(grid), the bandwidth-bound pass
-//   3. link_cells     (only with a surface)   O(boundary cells)
+//   3. link_cells     (only with a surface)   O(boundary cells), after 1 and 2
 //   4. finalize_forces(only with a surface)   O(vertices)
 // then the host flips the current buffer, exactly where the reference calls
 // flow_field.swapMoments() (FsiCoupling2D.cu:419, FsiCoupling3D.cu:476).
@@ -41,6 +42,10 @@ struct ffs_lbm {
     LinkTable lt;
     float *staging = nullptr; // ncell * NM floats, allocated on first host transfer
     int dense_variant = -1;   // D3Q27 kernel variant chosen on the first step (tune_dense3d)
+    // link detection runs on `side` while the dense pass runs on the caller's
+    // stream; fork/join order them
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     // host-buffer step (ffs_lbm_step_host)
     float *hs_dev = nullptr;   // vertices | velocities | forces
     uint32_t *hs_elem = nullptr;
@@ -216,24 +221,31 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const ffs_surfac
     SurfaceArgs sa = surface_args(s);
     StepScalars sc{h->cl, h->ct, h->cf};
     uint32_t *words = reinterpret_cast<uint32_t *>(h->flags);
+    if (DIM == 3 && h->dense_variant < 0) h->dense_variant = tune_dense3d<T>(g, st);
     if (surf) {
         if (h->lt.cap == 0 || (int64_t)h->lt.acc_cap < s->num_vertices) {
             ffs_status r = ensure_links(h, std::max<int64_t>(s->num_vertices, h->lt.acc_cap),
                                         std::max<int64_t>(default_link_cells(h, s), h->lt.cap / 2));
             if (r != FFS_OK) return r;
         }
-        StageTimer t(h, 0, st);
-        FFS_CK((launch_detect_links<DIM, T>(g, words, h->lt, sa, sc, st)));
+        // Link detection and the dense pass overlap: the dense pass skips
+        // cells whose LINK bit it sees, but any link cell it does update is
+        // rewritten by link_cells, which runs after both.
+        FFS_CK(cudaEventRecord(h->fork, st));
+        FFS_CK(cudaStreamWaitEvent(h->side, h->fork, 0));
+        {
+            StageTimer t(h, 0, h->side);
+            FFS_CK((launch_detect_links<DIM, T>(g, words, h->lt, sa, sc, h->side)));
+        }
+        FFS_CK(cudaEventRecord(h->join, h->side));
     }
     {
         StageTimer t(h, 1, st);
         if (DIM == 2) FFS_CK(launch_dense2d<T>(g, st));
-        else {
-            if (h->dense_variant < 0) h->dense_variant = tune_dense3d<T>(g, st);
-            FFS_CK(launch_dense3d<T>(g, st, h->dense_variant));
-        }
+        else FFS_CK(launch_dense3d<T>(g, st, h->dense_variant));
     }
     if (surf) {
+        FFS_CK(cudaStreamWaitEvent(st, h->join, 0));
         {
             StageTimer t(h, 2, st);
             FFS_CK((launch_link_cells<DIM, T>(g, words, h->lt, sa, sc, st)));
@@ -396,6 +408,9 @@ ffs_status ffs_lbm_create(const ffs_lbm_desc *desc, ffs_lbm **out)
     if ((e = cudaMalloc(&h->flags, fbytes)) != cudaSuccess) return bail(e, "flags");
     if ((e = cudaMalloc(&h->wallmask, sizeof(uint32_t) * (size_t)ncell)) != cudaSuccess) return bail(e, "wallmask");
     if ((e = cudaMalloc(&h->status, sizeof(uint32_t))) != cudaSuccess) return bail(e, "status");
+    if ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    if ((e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+    if ((e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
     if ((e = cudaMemset(h->mom[0], 0, mbytes)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemset(h->mom[1], 0, mbytes)) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemset(h->flags, 0, fbytes)) != cudaSuccess) return bail(e, "memset");
@@ -416,6 +431,10 @@ ffs_status ffs_lbm_destroy(ffs_lbm *h)
     if (!h) return FFS_OK;
     for (auto &m : h->marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
     for (auto e : h->event_pool) cudaEventDestroy(e);
+    if (h->side) cudaStreamSynchronize(h->side);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    if (h->side) cudaStreamDestroy(h->side);
     cudaFree(h->mom[0]); cudaFree(h->mom[1]); cudaFree(h->flags); cudaFree(h->wallmask); cudaFree(h->status);
     cudaFree(h->staging); cudaFree(h->hs_dev); cudaFree(h->hs_elem);
     if (h->hs_pinned) cudaFreeHost(h->hs_pinned);
