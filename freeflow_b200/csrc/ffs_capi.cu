@@ -46,11 +46,6 @@ struct ffs_lbm {
     // stream; fork/join order them
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
-    // host-buffer step (ffs_lbm_step_host)
-    float *hs_dev = nullptr;   // vertices | velocities | forces
-    uint32_t *hs_elem = nullptr;
-    float *hs_pinned = nullptr; // forces readback
-    int hs_nv = 0, hs_ne = 0;
     // stage timing (ffs_lbm_profile_*)
     bool profiling = false;
     struct Mark { int stage; cudaEvent_t a, b; };
@@ -436,8 +431,7 @@ ffs_status ffs_lbm_destroy(ffs_lbm *h)
     if (h->join) cudaEventDestroy(h->join);
     if (h->side) cudaStreamDestroy(h->side);
     cudaFree(h->mom[0]); cudaFree(h->mom[1]); cudaFree(h->flags); cudaFree(h->wallmask); cudaFree(h->status);
-    cudaFree(h->staging); cudaFree(h->hs_dev); cudaFree(h->hs_elem);
-    if (h->hs_pinned) cudaFreeHost(h->hs_pinned);
+    cudaFree(h->staging);
     free_links(h->lt);
     delete h;
     return FFS_OK;
