@@ -49,3 +49,33 @@ def test_invalid_descriptor_is_rejected_without_gpu_work():
     assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
     assert b"dim" in L.ffs_last_error()
     assert L.ffs_lbm_create(None, ctypes.byref(h)) == 1
+
+
+def test_oversized_and_malformed_grids_are_rejected_before_any_device_work():
+    L = _capi.load()
+    h = ctypes.c_void_p()
+    d = _capi.LbmDesc()
+    d.dim, d.nx, d.ny, d.nz = 3, 2048, 2048, 1024       # 2^32 cells
+    d.fluid_viscosity, d.fluid_dx, d.dt = 0.01, 1.0, 1.0
+    assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 5   # FFS_ERR_UNSUPPORTED
+    assert b"2^31" in L.ffs_last_error()
+    d.nx = 0
+    assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.nx, d.nz, d.fluid_viscosity = 8, 8, 0.0
+    assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.fluid_viscosity, d.storage = 0.01, 7
+    assert L.ffs_lbm_create(ctypes.byref(d), ctypes.byref(h)) == 1
+
+
+def test_pool_descriptor_checks_need_no_device():
+    L = _capi.load()
+    h = ctypes.c_void_p()
+    d = _capi.PoolDesc()
+    d.storage, d.budget_bytes, d.max_episodes, d.substeps, d.num_actions = 1, 1 << 20, 0, 10, 8
+    assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.max_episodes, d.substeps = 4, 65
+    assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.substeps, d.num_actions = 10, 17
+    assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.num_actions, d.budget_bytes = 8, 0
+    assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
