@@ -88,28 +88,42 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
             int hi = min(__float2int_rz(geom::dvd(bmax[k], cl)) + 1, n3[k] - 1);
             ext[k] = max(hi - lo[k] + 1, 0);
         }
-        const int ncells = ext[0] * ext[1] * ext[2];
-        const int items = ncells * (Q - 1);
-        for (int it = lane; it < items; it += 32) {
-            const int l = it % (Q - 1) + 1;
-            const int c = it / (Q - 1);
-            const int i = lo[0] + c % ext[0];
-            const int j = lo[1] + (c / ext[0]) % ext[1];
-            const int k3 = lo[2] + c / (ext[0] * ext[1]);
+        const long long items = (long long)ext[0] * ext[1] * ext[2] * (Q - 1);
+        if (items == 0) continue;
+        // item it = cell * 26 + (l - 1), cell = (i - lo0) + ext0 * ((j - lo1) + ext1 * (k - lo2)).
+        // A lane steps by 32 items = one cell and 6 directions, so the cell
+        // and direction are carried forward instead of divided out.
+        int l = lane % (Q - 1) + 1;
+        int ci = 0, cj = 0, ck = 0;
+        auto advance = [&](int dc) {
+            ci += dc;
+            while (ci >= ext[0]) { ci -= ext[0]; ++cj; }
+            while (cj >= ext[1]) { cj -= ext[1]; ++ck; }
+        };
+        advance(lane / (Q - 1));
+        for (long long it = lane; it < items; it += 32) {
+            if (it != lane) {
+                l += 32 - (Q - 1);
+                int dc = 1;
+                if (l > Q - 1) { l -= Q - 1; dc = 2; }
+                advance(dc);
+            }
+            const int i = lo[0] + ci, j = lo[1] + cj, k3 = lo[2] + ck;
             int cx, cy, cz;
             dir_vec<3>(l, cx, cy, cz);
             // prefilter in ordinary (fast) float math; it only rejects clear
-            // misses: the plane is not reached (t outside [0, 1] by more than a
-            // margin of 2e-3 cells) or the plane point lies outside the
+            // misses: the plane is not reached (t = s1 / a outside [0, 1] by
+            // more than a margin of 2e-3 cells, tested as s1 sign(a) against
+            // [-margin, |a| + margin]) or the plane point lies outside the
             // triangle by more than 1% in barycentric terms
             const float px = (float)i * cl - tr.v0[0], py = (float)j * cl - tr.v0[1], pz = (float)k3 * cl - tr.v0[2];
             const float s1 = tr.n[0] * px + tr.n[1] * py + tr.n[2] * pz;
             const float a = cl * (tr.n[0] * cx + tr.n[1] * cy + tr.n[2] * cz);
             const float fa = fabsf(a);
             if (fa > margin) {
+                const float sa = a > 0.0f ? s1 : -s1;
+                if (sa < -margin || sa > fa + margin) continue;
                 const float t = __fdividef(s1, a);
-                const float tol = __fdividef(margin, fa);
-                if (t < -tol || t > 1.0f + tol) continue;
                 // plane point relative to v0: p1 - t c cl - v0
                 const float tc = t * cl;
                 const float wx = px - tc * cx, wy = py - tc * cy, wz = pz - tc * cz;
