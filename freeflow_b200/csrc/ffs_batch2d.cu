@@ -139,21 +139,25 @@ template <typename T>
 __global__ void __launch_bounds__(256, 3) pool_link_cells_kernel(const PoolEpisode *eps, LinkTable lt,
                                                                  const uint32_t *owner, int parity)
 {
-    constexpr int Q = 9;
-    const int lane = threadIdx.x & 31;
+    constexpr int Q = 9, G = kLinkGroup<2>, kPerWarp = 32 / G;
+    const int lane = threadIdx.x & (G - 1);
+    const uint32_t group = (threadIdx.x & 31) / G;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t n = *lt.count;
-    for (uint32_t w = ((blockIdx.x * blockDim.x) + threadIdx.x) >> 5; w < n; w += nwarps) {
-        const uint32_t slot = lt.list[w];
+    for (uint32_t w = (((blockIdx.x * blockDim.x) + threadIdx.x) >> 5) * kPerWarp; w < n; w += nwarps * kPerWarp) {
+        // two cells per warp, possibly of different episodes; a group past the
+        // end of the list rides along on the first group's cell
+        const bool valid = w + group < n;
+        const uint32_t slot = lt.list[valid ? w + group : w];
         const PoolEpisode &e = eps[owner[slot]];
         const uint32_t cell = lt.keys[slot] - 1 - e.cell_base;
         const GridArgs<T> g = episode_args<T>(e, parity);
         const SurfaceArgs sa = episode_surface(e);
         const StepScalars sc{e.cl, e.ct, e.cf};
-        link_cell_update<2, T, false>(g, lt.links, slot, cell, e.acc, sa, sc);
-        if (lane < Q) lt.links[(size_t)slot * Q + lane] = ~0ull;
+        link_cell_update<2, T, false>(g, lt.links, slot, cell, e.acc, sa, sc, valid);
+        if (valid && lane < Q) lt.links[(size_t)slot * Q + lane] = ~0ull;
         __syncwarp();
-        if (lane == 0) {
+        if (valid && lane == 0) {
             lt.keys[slot] = 0;
             set_link_bit(reinterpret_cast<uint32_t *>(e.flags), cell, false);
         }
@@ -289,6 +293,15 @@ template <typename T> int pool_dense_blocks_per_sm(int shape)
     return blocks;
 }
 
+template <typename T> int pool_link_cells_blocks_per_sm()
+{
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pool_link_cells_kernel<T>, 256, 0) != cudaSuccess ||
+        blocks < 1)
+        blocks = 1;
+    return blocks;
+}
+
 template <typename T>
 cudaError_t launch_pool_link_cells(const PoolEpisode *eps, const LinkTable &lt, const uint32_t *owner, int parity,
                                    int grid, cudaStream_t st)
@@ -316,6 +329,7 @@ cudaError_t launch_pool_outputs(const PoolEpisode *eps, const PoolActive *act, P
                                                int, int, cudaStream_t);                                                \
     template cudaError_t launch_pool_dense<T>(const PoolEpisode *, const PoolActive *, int, int, int, cudaStream_t);   \
     template int pool_dense_blocks_per_sm<T>(int);                                                                     \
+    template int pool_link_cells_blocks_per_sm<T>();                                                                   \
     template cudaError_t launch_pool_link_cells<T>(const PoolEpisode *, const LinkTable &, const uint32_t *, int, int, \
                                                    cudaStream_t);
 FFS_INST_POOL(float)

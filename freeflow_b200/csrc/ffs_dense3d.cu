@@ -55,48 +55,6 @@ __device__ __forceinline__ int ring_cell(int r)
     return hy * kHX + ((q < 8) ? 0 : kHX - 1);
 }
 
-// a0 + a1*c + a2*g(c) for a runtime c in {-1, 0, 1} (g = 1 or -1/2); the same
-// roundings as the matching output of herm3v: (a0 + a2) +- a1, or
-// fma(-1/2, a2, a0) for c = 0
-__device__ __forceinline__ float herm3_at(float a0, float a1, float a2, float c, float gc)
-{
-    return fmaf(c, a1, fmaf(gc, a2, a0));
-}
-
-// The three populations of one ring cell that the tile pulls: c_z slice kz
-// (runtime, one slice per thread), on the line ky = k of a ring row (the row
-// below the tile feeds c_y = +1, the row above c_y = -1) or kx = k of a ring
-// column.  sink(ky, kx, value); the values equal those of populations_each.
-template <typename Sink>
-__device__ __forceinline__ void ring_line(const Coef3V<float> &cf, int kz, bool row, int k, Sink &&sink)
-{
-    const float cz = (float)(kz - 1), gz = kz == 1 ? -0.5f : 1.0f, wz = wgt1(kz);
-    const float B00 = herm3_at(cf.rho, cf.m1z, cf.m2zz, cz, gz);
-    const float B10 = herm3_at(cf.m1x, cf.m2xz, cf.qxzz, cz, gz);
-    const float B01 = herm3_at(cf.m1y, cf.m2yz, cf.qyzz, cz, gz);
-    const float B20 = fmaf(cz, cf.qxxz, cf.m2xx);
-    const float B02 = fmaf(cz, cf.qyyz, cf.m2yy);
-    const float B11 = fmaf(cz, cf.qxyz, cf.m2xy);
-    if (row) {
-        const float cy = (float)(k - 1), gy = k == 1 ? -0.5f : 1.0f, wy = wgt1(k);
-        const float C0 = herm3_at(B00, B01, B02, cy, gy);
-        const float C1 = herm3_at(B10, B11, cf.qxyy, cy, gy);
-        const float C2 = fmaf(cy, cf.qxxy, B20);
-        float F[3];
-        herm3v(C0, C1, C2, F);
-#pragma unroll
-        for (int kx = 0; kx < 3; ++kx) sink(k, kx, ((wgt1(kx) * wy) * wz) * F[kx]);
-    } else {
-        const float cx = (float)(k - 1), gx = k == 1 ? -0.5f : 1.0f, wx = wgt1(k);
-        float C0[3], C1[3], C2[3];
-        herm3v(B00, B01, B02, C0);
-        herm3v(B10, B11, cf.qxyy, C1);
-        herm2v(B20, cf.qxxy, C2);
-#pragma unroll
-        for (int ky = 0; ky < 3; ++ky) sink(ky, k, ((wx * wgt1(ky)) * wz) * herm3_at(C0[ky], C1[ky], C2[ky], cx, gx));
-    }
-}
-
 // raw-moment slot: {rho, jx, jy, jz, Pxx, Pyy, Pzz, Pxy, Pyz, Pxz}
 // 9 populations of one c_z slice (clamped) -> x/y moments
 // Y = {Y00, Y01, Y02, Y10, Y11, Y20}
@@ -203,12 +161,7 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
 
 // MINB = CTAs per SM the register budget is cut for; launch_dense3d times the
 // variants on the grid and keeps the faster (tune_dense3d).
-// SPLIT: the ring cells are shared out three threads each, one c_z slice per
-// thread, and each thread evaluates only the three populations of its slice
-// that the tile pulls (ring_line), so 252 threads carry the ring work instead
-// of 84 threads each reconstructing whole ring cells while the others wait at
-// the plane barrier.  Slots of a ring cell that no tile cell pulls stay unset.
-template <typename T, int MINB, bool SPLIT>
+template <typename T, int MINB>
 __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T> g, int zchunk)
 {
     extern __shared__ float smem[];
@@ -224,15 +177,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     const bool inside = x < g.nx && y < g.ny;
     const int c_own = (ty + 1) * kHX + (tx + 1);
     // partner cell of the reconstruction pair
-    constexpr int kRingThreads = SPLIT ? 3 * kRing : kRing;
-    static_assert(kRingThreads <= D3::kThreads, "ring work needs partner threads");
-    const bool has_ring = tid < kRingThreads;
-    const int ring_id = SPLIT ? tid / 3 : tid;
-    const int c_ring = has_ring ? ring_cell(ring_id) : c_own;
-    // SPLIT: this thread's c_z slice of its ring cell, and the line it feeds
-    const int ring_kz = tid - 3 * ring_id;
-    const bool ring_row = ring_id < 2 * kHX;
-    const int ring_k = ring_row ? (c_ring < kHX ? 2 : 0) : (c_ring % kHX == 0 ? 2 : 0);
+    const bool has_ring = tid < kRing;
+    const int c_ring = has_ring ? ring_cell(tid) : c_own;
     auto planar = [&](int c) {
         int hx = c % kHX, hy = c / kHX;
         return (uint32_t)(halo_index(y0 + hy - 1, g.ny, wy) * g.nx + halo_index(x0 + hx - 1, g.nx, wx));
@@ -285,27 +231,9 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         cf.make(m);
         cf.populations_each([&](int kz, int ky, int kx, float v) { buf[set_of(kx, ky, kz) * kHalo + c] = v; });
     };
-    auto recon_ring_line = [&](float *buf) {
-        float *slice = buf + ring_kz * 9 * kHalo + c_ring;
-        if (is_bounce_back<3>(hB)) {
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int ky = ring_row ? ring_k : j, kx = ring_row ? j : ring_k;
-                slice[(ky * 3 + kx) * kHalo] = 0.0f;
-            }
-            return;
-        }
-        decode_moments<3, T>(mB, g.codec);
-        Coef3V<float> cf;
-        cf.make(mB);
-        ring_line(cf, ring_kz, ring_row, ring_k, [&](int ky, int kx, float v) { slice[(ky * 3 + kx) * kHalo] = v; });
-    };
     auto recon_plane = [&](float *buf) {
         recon_cell(buf, mA, hA, c_own);
-        if (has_ring) {
-            if constexpr (SPLIT) recon_ring_line(buf);
-            else recon_cell(buf, mB, hB, c_ring);
-        }
+        if (has_ring) recon_cell(buf, mB, hB, c_ring);
     };
     auto flag_at = [&](int z) -> uint32_t {
         return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[(size_t)z * nxy + col] : 0u;
@@ -404,19 +332,19 @@ static int choose_zchunks(int tiles, int nz, int slots)
     return best;
 }
 
-template <typename T, int MINB, bool SPLIT = false> struct Dense3dLaunch {
+template <typename T, int MINB> struct Dense3dLaunch {
     static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
     {
         static bool configured = false;
         static int slots = 0;
         if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(dense3d_kernel<T, MINB, SPLIT>,
+            cudaError_t e = cudaFuncSetAttribute(dense3d_kernel<T, MINB>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D3::kSmemBytes);
             if (e != cudaSuccess) return e;
             int dev = 0, sms = 0, per_sm = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense3d_kernel<T, MINB, SPLIT>, D3::kThreads,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense3d_kernel<T, MINB>, D3::kThreads,
                                                           D3::kSmemBytes);
             slots = sms * (per_sm > 0 ? per_sm : 1);
             configured = true;
@@ -425,7 +353,7 @@ template <typename T, int MINB, bool SPLIT = false> struct Dense3dLaunch {
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
         dim3 grid(tx, ty, (g.nz + zchunk - 1) / zchunk);
-        dense3d_kernel<T, MINB, SPLIT><<<grid, D3::kThreads, D3::kSmemBytes, s>>>(g, zchunk);
+        dense3d_kernel<T, MINB><<<grid, D3::kThreads, D3::kSmemBytes, s>>>(g, zchunk);
         return cudaGetLastError();
     }
 };
@@ -748,11 +676,7 @@ cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
     if constexpr (std::is_same<T, float>::value) {
         if (variant == 2) return Dense3dPairLaunch<2>::run(g, s);
     }
-    switch (variant) {
-    case 1: return Dense3dLaunch<T, 3>::run(g, s);
-    case 3: return Dense3dLaunch<T, 2, true>::run(g, s);
-    default: return Dense3dLaunch<T, 2>::run(g, s);
-    }
+    return variant == 1 ? Dense3dLaunch<T, 3>::run(g, s) : Dense3dLaunch<T, 2>::run(g, s);
 }
 
 // Times each variant on this grid (the pass only reads src and writes dst, so
@@ -779,7 +703,10 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
         cudaEventSynchronize(b);
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, a, b);
-        if (ms < best) { best = ms; best_v = v; }
+        // a later variant must win clearly: the variants may differ in the
+        // last bit of a result, and a pick decided by timing noise would make
+        // two runs of the same grid differ
+        if (ms < (v == 0 ? 1.0f : 0.97f) * best) { best = ms; best_v = v; }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);

@@ -37,6 +37,10 @@ __device__ __forceinline__ float line_isect(float x1, float y1, float x2, float 
 {
     float a1 = sub(mul(sub(x1, x2), sub(y3, y4)), mul(sub(y1, y2), sub(x3, x4)));
     float b1 = sub(mul(sub(x4, x2), sub(y3, y4)), mul(sub(y4, y2), sub(x3, x4)));
+    // t1 = b1 / a1 can only land in (0, 1) when b1 and a1 have the same sign,
+    // b1 != 0 and |b1| < |a1|; every other case (a1 = 0 and NaN included)
+    // ends in the -1 below as well, so reject it before dividing
+    if (!(fabsf(b1) < fabsf(a1)) || b1 == 0.0f || ((b1 < 0.0f) != (a1 < 0.0f))) return -1.0f;
     if (fabsf(a1) <= 0.0f) return -1.0f;
     float t1 = dvd(b1, a1);
     if (t1 <= 0.0f || t1 >= 1.0f) return -1.0f;

@@ -14,7 +14,8 @@
 //               atomicMin keeps the nearest (depth, element) key.  The owning
 //               cell gets a LINK bit in its flag byte, so the dense kernels
 //               skip it.  Nothing proportional to the grid is touched.
-//   link cells  one warp per link-owning cell, lane i = direction i: wall
+//   link cells  one warp per D3Q27 link-owning cell (half a warp per D2Q9
+//               cell), lane i = direction i: wall
 //               bounce-back, moving-wall reconstruction with the momentum
 //               exchange force, or the ordinary pull (reconstructing the
 //               neighbour's population from its moments).  The warp reduces
@@ -44,6 +45,20 @@ static int sm_count()
         if (n <= 0) n = 148;
     }
     return n;
+}
+
+// CTAs of `threads` threads of KERNEL that are resident on the device at
+// once (no dynamic shared memory); computed once per kernel.
+template <auto KERNEL> static int resident_grid(int threads)
+{
+    static int grid = 0;
+    if (!grid) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERNEL, threads, 0) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        grid = sm_count() * per_sm;
+    }
+    return grid;
 }
 
 // D3Q27: one warp per triangle.  The triangle's own geometry is evaluated
@@ -161,18 +176,21 @@ template <int DIM, typename T, bool HALF>
 __global__ void __launch_bounds__(256, 3) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
                                                          StepScalars sc)
 {
-    constexpr int Q = Lattice<DIM>::Q;
-    const int lane = threadIdx.x & 31;
+    constexpr int Q = Lattice<DIM>::Q, G = kLinkGroup<DIM>, kPerWarp = 32 / G;
+    const int lane = threadIdx.x & (G - 1);
+    const uint32_t group = (threadIdx.x & 31) / G;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t n = *lt.count;
-    for (uint32_t w = ((blockIdx.x * blockDim.x) + threadIdx.x) >> 5; w < n; w += nwarps) {
-        const uint32_t slot = lt.list[w];
+    for (uint32_t w = (((blockIdx.x * blockDim.x) + threadIdx.x) >> 5) * kPerWarp; w < n; w += nwarps * kPerWarp) {
+        // a group past the end of the list rides along on the first group's cell
+        const bool valid = w + group < n;
+        const uint32_t slot = lt.list[valid ? w + group : w];
         const uint32_t cell = lt.keys[slot] - 1;
-        link_cell_update<DIM, T, HALF>(g, lt.links, slot, cell, lt.acc, s, sc);
+        link_cell_update<DIM, T, HALF>(g, lt.links, slot, cell, lt.acc, s, sc, valid);
         // return the slot to the empty state and drop the cell's LINK bit
-        if (lane < Q) lt.links[(size_t)slot * Q + lane] = ~0ull;
+        if (valid && lane < Q) lt.links[(size_t)slot * Q + lane] = ~0ull;
         __syncwarp();
-        if (lane == 0) {
+        if (valid && lane == 0) {
             lt.keys[slot] = 0;
             set_link_bit(flag_words, cell, false);
         }
@@ -235,12 +253,15 @@ template <int DIM, typename T>
 cudaError_t launch_link_cells(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
                               const StepScalars &sc, cudaStream_t st)
 {
-    // persistent warps over the device-side count: 8 warps per CTA, 4 CTAs per SM
-    int grid = sm_count() * 4;
+    // persistent warps over the device-side count, one wave: as many CTAs of
+    // 8 warps as are resident together (a CTA beyond that would run its fixed
+    // share of the cells after the others finish)
     if (g.half_pops)
-        link_cells_kernel<DIM, T, true><<<grid, 256, 0, st>>>(g, flag_words, lt, s, sc);
+        link_cells_kernel<DIM, T, true><<<resident_grid<link_cells_kernel<DIM, T, true>>(256), 256, 0, st>>>(
+            g, flag_words, lt, s, sc);
     else
-        link_cells_kernel<DIM, T, false><<<grid, 256, 0, st>>>(g, flag_words, lt, s, sc);
+        link_cells_kernel<DIM, T, false><<<resident_grid<link_cells_kernel<DIM, T, false>>(256), 256, 0, st>>>(
+            g, flag_words, lt, s, sc);
     return cudaGetLastError();
 }
 

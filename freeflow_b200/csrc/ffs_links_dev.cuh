@@ -123,12 +123,15 @@ __device__ __forceinline__ void detect_pair(const GridArgs<T> &g, uint32_t *flag
 // atomic.  Integer sums are associative, so the per-vertex result does not
 // depend on warp, lane or launch order.  A share beyond +-127 lattice units
 // (outside the 2^-24 range of 27 summed int32 shares) is clamped and flagged.
+// Lanes are grouped by (lane group, element): the groups of one warp may
+// update cells of different grids, whose element numbers name different
+// elements and whose accumulators differ.
 template <int DIM>
 __device__ __forceinline__ void add_forces_warp(long long *acc, bool active, uint32_t elem, const uint32_t *vert,
-                                                const float (*share)[3], uint32_t *status)
+                                                const float (*share)[3], uint32_t *status, uint32_t group = 0)
 {
     const unsigned full = 0xffffffffu;
-    const unsigned peers = __match_any_sync(full, active ? elem : 0xffffffffu);
+    const unsigned peers = __match_any_sync(full, active ? ((unsigned long long)group << 32) | elem : ~0ull);
     const int lane = threadIdx.x & 31;
     const bool leader = active && lane == __ffs(peers) - 1;
 #pragma unroll
@@ -148,18 +151,27 @@ __device__ __forceinline__ void add_forces_warp(long long *acc, bool active, uin
         }
 }
 
-// Update of one link-owning cell by one warp (lane i = direction i): wall
-// bounce-back, moving-wall reconstruction with its momentum-exchange force
-// shares, or the ordinary pull; the raw moments are reduced across the
-// warp and lane 0 collides, stores and feeds outlets.  `links` holds the
-// Q keys of the cell's table slot; the force shares go to `acc`.
+// Lanes per link cell: a D3Q27 cell takes a whole warp, a D2Q9 cell half of
+// one, so a warp updates two D2Q9 cells at once.
+template <int DIM> constexpr int kLinkGroup = DIM == 2 ? 16 : 32;
+
+// Update of one link-owning cell by one lane group of kLinkGroup<DIM> lanes
+// (lane i of the group = direction i): wall bounce-back, moving-wall
+// reconstruction with its momentum-exchange force shares, or the ordinary
+// pull; the raw moments are reduced across the group and its lane 0
+// collides, stores and feeds outlets.  `links` holds the Q keys of the
+// cell's table slot; the force shares go to `acc`.  Every lane of the warp
+// calls this together (the force sums and the reduction are warp-wide); a
+// group with valid = false has no cell this round and only takes part in
+// those, with arguments that still name a real cell.
 template <int DIM, typename T, bool HALF>
 __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const unsigned long long *links,
                                                  uint32_t slot, uint32_t cell, long long *acc,
-                                                 const SurfaceArgs &s, const StepScalars &sc)
+                                                 const SurfaceArgs &s, const StepScalars &sc, bool valid = true)
 {
-    constexpr int Q = Lattice<DIM>::Q, NM = Lattice<DIM>::NM;
-    const int lane = threadIdx.x & 31;
+    constexpr int Q = Lattice<DIM>::Q, NM = Lattice<DIM>::NM, G = kLinkGroup<DIM>;
+    static_assert(Q <= G, "one lane per direction");
+    const int lane = threadIdx.x & (G - 1);
     const unsigned full = 0xffffffffu;
     const long long nxy = (long long)g.nx * g.ny;
     const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
@@ -167,16 +179,17 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
     const int y = (int)((cell / g.nx) % g.ny);
     const int z = (int)(cell / nxy);
     const uint8_t f8 = g.flags[cell];
-    if (is_updated(f8 & kTypeMask)) {
-        float mc[NM];
+    const bool upd = valid && is_updated(f8 & kTypeMask);
+    float mc[NM];
+    float pop = 0.0f;
+    bool has_share = false;
+    uint32_t hit_elem = 0xffffffffu;
+    uint32_t vshare[3] = {0, 0, 0};
+    float share[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; // [vertex][component]
+    if (upd) {
         load_moments<DIM, T>(mc, g.src, g.ncell, cell, g.codec);
         Coef<DIM> own;
         own.make(mc);
-        float pop = 0.0f;
-        bool has_share = false;
-        uint32_t hit_elem = 0xffffffffu;
-        uint32_t vshare[3] = {0, 0, 0};
-        float share[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; // [vertex][component]
         if (lane < Q) {
             const int i = lane;
             int cx, cy, cz;
@@ -263,25 +276,28 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
                 pop = fmaxf(v, 0.0f);
             }
         }
-        // forces: one share per (link, element vertex), summed per element
-        add_forces_warp<DIM>(acc, has_share, hit_elem, vshare, share, g.status);
-        // raw moments by warp reduction
-        int cx = 0, cy = 0, cz = 0;
-        if (lane < Q) dir_vec<DIM>(lane, cx, cy, cz);
-        const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
-        float R[NM];
-        if (DIM == 2) {
-            R[0] = pop; R[1] = pop * fx; R[2] = pop * fy;
-            R[3] = pop * fx * fx; R[4] = pop * fy * fy; R[5] = pop * fx * fy;
-        } else {
-            R[0] = pop; R[1] = pop * fx; R[2] = pop * fy; R[3] = pop * fz;
-            R[4] = pop * fx * fx; R[5] = pop * fy * fy; R[6] = pop * fz * fz;
-            R[7] = pop * fx * fy; R[8] = pop * fy * fz; R[9] = pop * fx * fz;
-        }
+    }
+    // forces: one share per (link, element vertex), summed per element
+    add_forces_warp<DIM>(acc, has_share, hit_elem, vshare, share, g.status, (threadIdx.x & 31) / G);
+    // raw moments by reduction within the group (lanes Q.. add exact zeros,
+    // so the sums equal those of a whole-warp reduction)
+    int cx = 0, cy = 0, cz = 0;
+    if (lane < Q) dir_vec<DIM>(lane, cx, cy, cz);
+    const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
+    float R[NM];
+    if (DIM == 2) {
+        R[0] = pop; R[1] = pop * fx; R[2] = pop * fy;
+        R[3] = pop * fx * fx; R[4] = pop * fy * fy; R[5] = pop * fx * fy;
+    } else {
+        R[0] = pop; R[1] = pop * fx; R[2] = pop * fy; R[3] = pop * fz;
+        R[4] = pop * fx * fx; R[5] = pop * fy * fy; R[6] = pop * fz * fz;
+        R[7] = pop * fx * fy; R[8] = pop * fy * fz; R[9] = pop * fx * fz;
+    }
 #pragma unroll
-        for (int k = 0; k < NM; ++k)
+    for (int k = 0; k < NM; ++k)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) R[k] += __shfl_xor_sync(full, R[k], o);
+        for (int o = G / 2; o > 0; o >>= 1) R[k] += __shfl_xor_sync(full, R[k], o);
+    if (upd) {
         if (lane == 0) {
             float m[NM];
             if (DIM == 2) collide2(R, g.omega, m);

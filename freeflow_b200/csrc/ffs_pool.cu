@@ -194,6 +194,7 @@ struct ffs_pool {
     int64_t advances = 0, graph_builds = 0;
     int sms = 148;
     int grid_dense[kPoolNumShapes] = {};
+    int grid_link = 0;        // resident CTAs of the link-cell kernel (one wave)
 };
 
 namespace {
@@ -245,7 +246,7 @@ ffs_status wait_idle(ffs_pool *p)
 template <typename T> ffs_status capture(ffs_pool *p, int shape, int parity, cudaGraphExec_t *out)
 {
     const int S = p->d.substeps;
-    const int g_kin = p->sms * 4, g_det = p->sms * 8, g_link = p->sms * 4, g_fin = p->sms * 2;
+    const int g_kin = p->sms * 4, g_det = p->sms * 8, g_link = p->grid_link, g_fin = p->sms * 2;
     cudaGraph_t graph = nullptr;
     POOL_CK(cudaStreamBeginCapture(p->st, cudaStreamCaptureModeThreadLocal));
     cudaError_t err = cudaSuccess;
@@ -424,6 +425,11 @@ ffs_status ffs_pool_create(const ffs_pool_desc *desc, ffs_pool **out)
         default: b = pool_dense_blocks_per_sm<__nv_bfloat16>(sh); break;
         }
         p->grid_dense[sh] = p->sms * b;
+    }
+    switch (d.storage) {
+    case FFS_STORAGE_F32: p->grid_link = p->sms * pool_link_cells_blocks_per_sm<float>(); break;
+    case FFS_STORAGE_F16: p->grid_link = p->sms * pool_link_cells_blocks_per_sm<__half>(); break;
+    default: p->grid_link = p->sms * pool_link_cells_blocks_per_sm<__nv_bfloat16>(); break;
     }
     if ((e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
     if ((e = cudaEventCreate(&p->ev0)) != cudaSuccess) return bail(e, "event");

@@ -115,6 +115,8 @@ cudaError_t launch_pool_dense(const PoolEpisode *eps, const PoolActive *act, int
 template <typename T>
 int pool_dense_blocks_per_sm(int shape);
 template <typename T>
+int pool_link_cells_blocks_per_sm();
+template <typename T>
 cudaError_t launch_pool_link_cells(const PoolEpisode *eps, const LinkTable &lt, const uint32_t *owner, int parity,
                                    int grid, cudaStream_t st);
 cudaError_t launch_pool_finalize(const PoolEpisode *eps, const PoolActive *act, const LinkTable &lt, int grid,

@@ -2,9 +2,7 @@
 per grid by speed, so each must pass the parity cases on its own).
 
 Variants: 0 and 1 are the single-plane z-march built for two and three CTAs
-per SM; 2 is the pair kernel (two planes per step in f32x2, FP32 storage);
-3 is variant 0 with the halo-ring reconstruction shared out three threads per
-ring cell, one c_z slice each.
+per SM; 2 is the pair kernel (two planes per step in f32x2, FP32 storage).
 Tolerances are those of test_gpu_parity.py: 2e-6 against the ref32 oracle,
 4e-6 next to walls (bounce-back added as a correction), 5e-6 against FP64.
 """
@@ -17,7 +15,7 @@ from helpers import max_abs, run_pair
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [0, 1, 2, 3]
+VARIANTS = [0, 1, 2]
 
 
 @pytest.fixture(params=VARIANTS)
