@@ -311,7 +311,8 @@ def run_serving(iterations: int, warmup: int, concurrency: int = 256, plain_step
         "batched": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()},
         "plain_f32": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in plain.items()},
         "speedup_vs_plain": round(r["env_steps_per_s"] / plain["env_steps_per_s"], 2),
-        "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}", "graph_builds": info["graph_builds"],
+        "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}" + (" strip" if info["strip"] else ""),
+                 "graph_builds": info["graph_builds"],
                  "max_episodes": 2 * concurrency,
                  "dense_ms_at_tuning": round(info["dense_ms"], 4), "cells_at_tuning": info["tuned_cells"],
                  "dense_roofline": ({"achieved": round(dense_gbs, 1), "peak": peak, "unit": "GB/s",

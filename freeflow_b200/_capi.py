@@ -96,7 +96,7 @@ class PoolInfo(C.Structure):
     _fields_ = [("budget_bytes", C.c_int64), ("free_bytes", C.c_int64), ("largest_free_bytes", C.c_int64),
                 ("active_episodes", C.c_int), ("tiles", C.c_int), ("tile_x", C.c_int), ("tile_y", C.c_int),
                 ("advances", C.c_int64), ("graph_builds", C.c_int64), ("cells", C.c_int64),
-                ("tuned_cells", C.c_int64), ("dense_ms", C.c_double)]
+                ("tuned_cells", C.c_int64), ("dense_ms", C.c_double), ("strip", C.c_int), ("pad", C.c_int)]
 
 
 POOL_MAX_ACTIONS = 16

@@ -302,6 +302,23 @@ struct Vel6 {
 
 // --------------------------------------------------------- grid descriptor
 // Everything one fluid grid's kernels need, passed by value.
+// cp.async (LDGSTS): 4-byte global -> shared copies that hold no registers
+// while in flight.  Both addresses must be 4-byte aligned.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+// 16-byte copy (L2 only); both addresses must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// waits until at most N of this thread's committed groups are still in flight
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <typename T> struct GridArgs {
     int nx, ny, nz;
     uint32_t ncell;

@@ -52,6 +52,61 @@ __device__ __forceinline__ void dense2d_load(const GridArgs<T> &g, int x0, int y
     }
 }
 
+// Populations of one cell from its stored moments (reconstruction step of
+// the update); HALF rounds them to binary16 like the reference's __half tile.
+template <typename T, bool HALF>
+__device__ __forceinline__ void dense2d_recon(const GridArgs<T> &g, const T (&raw)[6], float (&f)[9])
+{
+    float m[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m[k] = StorageTraits<T>::from(raw[k]);
+    decode_moments<2, T>(m, g.codec);
+    Coef<2> cf;
+    cf.make(m);
+    cf.populations(f);
+    if (HALF) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = round_half(f[i]);
+    }
+}
+
+// Update of one cell that the dense pass owns (flag f8: Fluid or
+// SolidDynamic, no moving-boundary link): pull(i) is the reconstructed
+// population i of the upstream cell x - c_i and own(i) that of the cell
+// itself.  Bounce-back, clamp, raw moments, collision, store and the outlet
+// feed follow FsiCoupling2D.cu:154-252.
+template <typename T, typename Pull, typename Own>
+__device__ __forceinline__ void dense2d_update_cell(const GridArgs<T> &g, uint32_t idx, uint32_t f8, Pull &&pull,
+                                                    Own &&own)
+{
+    using L = Lattice<2>;
+    float pop[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) pop[i] = pull(i);
+    const uint32_t wm = (f8 & (kBitNearWall | kBitOutletSrc)) ? g.wallmask[idx] : 0u;
+    if (f8 & kBitNearWall) {
+        // bounce-back: f_i(x) = f_inv(i)^rec(x) when x - c_i is a wall
+#pragma unroll
+        for (int i = 1; i < 9; ++i)
+            if (wm & (1u << i)) pop[i] = own(L::inv(i));
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) pop[i] = fmaxf(pop[i], 0.0f);
+    float R[6], m[6];
+    raw_moments2(pop, R);
+    collide2(R, g.omega, m);
+    T *planes[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
+    encode_store<2, T>(m, planes, idx, g.codec);
+    if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
+    if (f8 & kBitOutletSrc) {
+        float ms[6];
+        stored_values<2, T>(m, ms, g.codec);
+        feed_outlets<2, T>(g, idx, ms, wm);
+    }
+}
+
 // Processes the TX x TY tile with lower-left cell (x0, y0) from the halo
 // moments `raw` (dense2d_load).  The caller's CTA has TX * TY threads; sp is
 // the CTA's population tile (tile + halo).  after_recon() runs once the halo
@@ -72,16 +127,10 @@ __device__ __forceinline__ void dense2d_tile_loaded(const GridArgs<T> &g, int x0
         const int c = tid + r * H::kThreads;
         if (c < H::kHalo) {
             const int hx = c % H::kHX, hy = c / H::kHX;
-            float m[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) m[k] = StorageTraits<T>::from(raw[r][k]);
-            decode_moments<2, T>(m, g.codec);
-            Coef<2> cf;
-            cf.make(m);
             float f[9];
-            cf.populations(f);
+            dense2d_recon<T, HALF>(g, raw[r], f);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) sp[i][hy][hx] = HALF ? round_half(f[i]) : f[i];
+            for (int i = 0; i < 9; ++i) sp[i][hy][hx] = f[i];
         }
     }
     after_recon();
@@ -92,33 +141,10 @@ __device__ __forceinline__ void dense2d_tile_loaded(const GridArgs<T> &g, int x0
     if (x < g.nx && y < g.ny) {
         const uint32_t idx = (uint32_t)(y * g.nx + x);
         const uint8_t f8 = g.flags[idx];
-        if (is_updated(f8 & kTypeMask) && !(f8 & kBitLink)) {
-            float pop[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) pop[i] = sp[i][ty + 1 - L::cy(i)][tx + 1 - L::cx(i)];
-            const uint32_t wm = (f8 & (kBitNearWall | kBitOutletSrc)) ? g.wallmask[idx] : 0u;
-            if (f8 & kBitNearWall) {
-                // bounce-back: f_i(x) = f_inv(i)^rec(x) when x - c_i is a wall
-#pragma unroll
-                for (int i = 1; i < 9; ++i)
-                    if (wm & (1u << i)) pop[i] = sp[L::inv(i)][ty + 1][tx + 1];
-            }
-#pragma unroll
-            for (int i = 0; i < 9; ++i) pop[i] = fmaxf(pop[i], 0.0f);
-            float R[6], m[6];
-            raw_moments2(pop, R);
-            collide2(R, g.omega, m);
-            T *planes[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
-            encode_store<2, T>(m, planes, idx, g.codec);
-            if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
-            if (f8 & kBitOutletSrc) {
-                float ms[6];
-                stored_values<2, T>(m, ms, g.codec);
-                feed_outlets<2, T>(g, idx, ms, wm);
-            }
-        }
+        if (is_updated(f8 & kTypeMask) && !(f8 & kBitLink))
+            dense2d_update_cell(
+                g, idx, f8, [&](int i) { return sp[i][ty + 1 - L::cy(i)][tx + 1 - L::cx(i)]; },
+                [&](int i) { return sp[i][ty + 1][tx + 1]; });
     }
 }
 

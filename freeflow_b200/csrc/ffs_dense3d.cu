@@ -380,13 +380,6 @@ constexpr int kStageOwn = 20 * D3::kThreads;   // 2 planes x 10 moments per tile
 constexpr int kStageRing = 20 * kRing;
 constexpr size_t kPairSmemBytes = (size_t)27 * kHalo * sizeof(f2) + (size_t)(kStageOwn + kStageRing) * sizeof(float);
 
-__device__ __forceinline__ void cp_async4(float *dst, const float *src)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ f2 lds_clamped(const f2 *buf, int idx)
 {
@@ -581,7 +574,7 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_pair_kernel(GridAr
     for (int k = 0; k < 10; ++k) A[k] = f2make(0.0f, 0.0f);
     types = issue_pair(zb - 1);
     for (int s = zb - 1; s <= ze; s += 2) {
-        cp_async_wait_all();
+        cp_async_wait<0>();
         recon_pair(st_own, D3::kThreads, types & 0xFF, (types >> 8) & 0xFF, c_own);
         if (has_ring) recon_pair(st_ring, kRing, (types >> 16) & 0xFF, types >> 24, c_ring);
         // the next pair's moments and types, the flags two planes ahead, this pair's masks

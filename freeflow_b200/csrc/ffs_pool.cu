@@ -16,10 +16,12 @@
 // reused for every mix.  The active table is re-uploaded only after the mix
 // changed; the per-step parameters (actions, wave phases) are one upload.
 //
-// Tile shape of the dense pass: ffs_pool_tune times the candidate shapes on
-// the current mix (CUDA events, a warm launch then five timed ones each) and
-// keeps the fastest.  It runs by itself on the first advance and again when
-// the number of cells has grown or shrunk by 2x since the last tuning.
+// Work unit of the dense pass: ffs_pool_tune times the candidate units
+// (tiles and row-marching strips, kPoolShapes) on the current mix (CUDA
+// events, a warm launch then five timed ones each) and keeps the fastest.
+// Every unit gives the same bits, so the choice changes only the speed.  It
+// runs by itself on the first advance and again when the number of cells has
+// grown or shrunk by 2x since the last tuning.  FFS_POOL_SHAPE pins the unit.
 //
 // Ordering: every device operation of a pool is issued on the pool's stream,
 // so an evicted episode's block is reused only after the work that read it.
@@ -27,6 +29,7 @@
 // has completed (ffs_pool_advance waits for it).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -270,12 +273,23 @@ template <typename T> ffs_status capture(ffs_pool *p, int shape, int parity, cud
     return FFS_OK;
 }
 
+// FFS_POOL_SHAPE pins the dense work unit (an index into kPoolShapes) for
+// tests that check every unit; -1 when unset or out of range.
+static int pinned_shape()
+{
+    const char *pin = std::getenv("FFS_POOL_SHAPE");
+    if (!pin) return -1;
+    const int v = std::atoi(pin);
+    return (v >= 0 && v < kPoolNumShapes) ? v : -1;
+}
+
 template <typename T> ffs_status tune_impl(ffs_pool *p)
 {
     if (p->order.empty()) return FFS_OK;
     float best = 1e30f;
     int best_shape = p->shape;
-    for (int sh = 0; sh < kPoolNumShapes; ++sh) {
+    const int pin = pinned_shape(); // a pinned shape is only timed
+    for (int sh = pin >= 0 ? pin : 0; sh < (pin >= 0 ? pin + 1 : kPoolNumShapes); ++sh) {
         p->shape = sh;
         ffs_status r = upload_active(p);
         if (r != FFS_OK) return r;
@@ -371,6 +385,7 @@ ffs_status ffs_pool_create(const ffs_pool_desc *desc, ffs_pool **out)
     ffs_pool *p = new (std::nothrow) ffs_pool();
     if (!p) return fail(FFS_ERR_OUT_OF_MEMORY, "host allocation failed");
     p->d = d;
+    if (pinned_shape() >= 0) p->shape = pinned_shape();
     p->esize = d.storage == FFS_STORAGE_F32 ? 4 : 2;
     p->slots.resize(d.max_episodes);
     auto bail = [&](cudaError_t e, const char *what) {
@@ -753,6 +768,7 @@ ffs_status ffs_pool_get_info(const ffs_pool *p, ffs_pool_info *info)
     info->tiles = (int)tiles;
     info->tile_x = sh.tx;
     info->tile_y = sh.ty;
+    info->strip = sh.strip ? 1 : 0;
     info->advances = p->advances;
     info->graph_builds = p->graph_builds;
     info->cells = mix_cells(p);

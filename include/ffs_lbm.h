@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 1
+#define FFS_ABI_VERSION 2
 
 typedef struct ffs_lbm ffs_lbm;
 

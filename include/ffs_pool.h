@@ -97,6 +97,9 @@ typedef struct {
     int64_t cells;             /* fluid cells over all admitted episodes */
     int64_t tuned_cells;       /* fluid cells of the mix at the last tuning */
     double dense_ms;           /* one dense pass over that mix (CUDA events, mean of 5) */
+    int strip;                 /* 1: the dense unit is a strip of tile_x columns and tile_y
+                                  rows walked row by row; 0: a tile_x x tile_y tile */
+    int pad;
 } ffs_pool_info;
 
 ffs_status ffs_pool_create(const ffs_pool_desc *desc, ffs_pool **out);

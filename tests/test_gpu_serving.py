@@ -8,6 +8,8 @@
   * FP16 storage vs the FP64 oracle: relative L2 velocity error <= 1e-3
     (closed tank; FP32 storage, for scale, <= 5e-4)
   * admission by device memory, eviction, and graph reuse across mixes
+The identity tests run once per dense work unit (FFS_POOL_SHAPE pins it): the
+five tile shapes and the three row-marching strips must all give the same bits.
 """
 import numpy as np
 import pytest
@@ -17,6 +19,15 @@ from freeflow_b200 import serving as S
 from helpers import max_abs
 
 pytestmark = pytest.mark.gpu
+
+TILES, STRIPS = [0, 1, 2, 3, 4], [5, 6, 7]
+
+
+@pytest.fixture
+def pin_shape(monkeypatch):
+    def pin(shape):
+        monkeypatch.setenv("FFS_POOL_SHAPE", str(shape))
+    return pin
 
 
 def _actions(sp, step):
@@ -36,7 +47,9 @@ def _run_pool(pool, slots_specs, control_steps):
     return outs
 
 
-def test_pool_f32_matches_single_grid_step(cuda):
+@pytest.mark.parametrize("shape", TILES + STRIPS)
+def test_pool_f32_matches_single_grid_step(cuda, pin_shape, shape):
+    pin_shape(shape)
     specs = [S.make_episode(256, 128, seed=11, length=10), S.make_episode(512, 192, seed=12, length=10)]
     pool = S.Pool(storage="f32", budget_bytes=1 << 30, max_episodes=8)
     slots = [(pool.admit(sp), sp) for sp in specs]
@@ -53,9 +66,11 @@ def test_pool_f32_matches_single_grid_step(cuda):
     pool.close()
 
 
-def test_pool_matches_oracle(cuda):
+@pytest.mark.parametrize("shape", [1] + STRIPS)
+def test_pool_matches_oracle(cuda, pin_shape, shape):
     from oracle.oracle import Oracle
 
+    pin_shape(shape)
     sp = S.make_episode(256, 128, seed=21, length=10)
     pool = S.Pool(storage="f32", budget_bytes=256 << 20, max_episodes=2)
     s = pool.admit(sp)
@@ -82,7 +97,33 @@ def test_pool_matches_oracle(cuda):
     pool.close()
 
 
-def test_episode_alone_and_in_mix_identical(cuda):
+@pytest.mark.parametrize("storage", ["f16", "f32"])
+def test_strip_and_tile_units_agree_on_odd_widths(cuda, pin_shape, storage):
+    """Odd row widths: 2-byte moments cannot be staged two per 4-byte copy, so
+    the strip kernel copies them one by one; walls on every side exercise the
+    bounce-back path of the strip kernel too."""
+    res = []
+    for sides in ("outlets", "walls"):
+        sp = S.make_episode(255, 131, seed=51, length=10, sides=sides)
+        for shape in (1, 5, 6):
+            pin_shape(shape)
+            pool = S.Pool(storage=storage, budget_bytes=256 << 20, max_episodes=2)
+            s = pool.admit(sp)
+            out = _run_pool(pool, [(s, sp)], 2)[s]
+            res.append((sides, out, pool.get_moments(s)))
+            pool.close()
+    for k in (0, 3):
+        for j in (1, 2):
+            (_, oa, ma), (_, ob, mb) = res[k], res[k + j]
+            for a, b in zip(oa, ob):
+                assert a[:5] == b[:5]
+                assert np.array_equal(a[5], b[5])
+            assert np.array_equal(ma, mb)
+
+
+@pytest.mark.parametrize("shape", [1] + STRIPS)
+def test_episode_alone_and_in_mix_identical(cuda, pin_shape, shape):
+    pin_shape(shape)
     target = S.make_episode(512, 192, seed=31, length=10)
     others = [S.make_episode(n[0], n[1], seed=40 + i, length=10)
               for i, n in enumerate([(256, 128), (1200, 400), (512, 192), (256, 128), (1200, 400)])]
