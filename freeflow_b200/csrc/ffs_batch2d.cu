@@ -135,33 +135,35 @@ __global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *
 }
 
 // ---------------------------------------------------------- dense (strips)
-// Row-marching variant of the dense pass.  A work unit is a strip of TX
+// Row-marching variant of the dense pass.  A work unit is a strip of TX-2
 // columns and CH rows of one episode; a CTA of TX threads walks up its rows:
-//   * the stored moments of each row (columns x0-P .. x0+TX+P-1, P = the
-//     cells of one 16-byte copy) are staged in shared memory by 16-byte
-//     cp.async copies DEPTH rows ahead of use, so the loads in flight hold no
-//     registers (rows whose width is not a multiple of P are copied cell by
-//     cell instead, since their copies would not start on 16-byte bounds);
-//   * each row is reconstructed once into a ring of four population rows
-//     (thread t takes column x0+t; threads 0 and TX-1 also take the x-halo
-//     cells x0-1 and x0+TX), so a unit reconstructs CH+2 rows for CH;
-//   * row o is updated from ring rows o-1, o, o+1 in the iteration after
-//     row o+1 was reconstructed, which leaves one barrier per row.
+//   * the stored moments of each row's TX halo cells (columns x0-1 ..
+//     x0+TX-2) are staged in shared memory by 16-byte cp.async copies DEPTH
+//     rows ahead of use, from a window that starts on a 16-byte bound, so the
+//     loads in flight hold no registers (rows whose width is not a multiple
+//     of a copy's cells are copied cell by cell instead);
+//   * each row is reconstructed once into a ring of four population rows,
+//     one halo cell per thread, so every thread does the same work and a
+//     unit reconstructs CH+2 rows for CH;
+//   * threads 1..TX-2 update row o from ring rows o-1, o, o+1 in the
+//     iteration after row o+1 was reconstructed, which leaves one barrier per
+//     row.
 // The per-cell arithmetic is dense2d_recon / dense2d_update_cell, the same
 // code as the tile kernel, so both give the same bits.
 template <typename T, int TX, int CH, int DEPTH>
 __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
 {
     using L = Lattice<2>;
-    constexpr int kDepth = DEPTH;           // rows staged ahead of use
-    constexpr int kStage = kDepth + 1;      // staging slots
-    constexpr int kRing = 4;                // population rows
-    constexpr int kPer = 16 / (int)sizeof(T); // cells per 16-byte copy (the pad P)
-    constexpr int kSW = TX + 2 * kPer;        // staged cells per row: x0-P .. x0+TX+P-1
+    constexpr int kOut = TX - 2;              // columns a strip updates
+    constexpr int kDepth = DEPTH;             // rows staged ahead of use
+    constexpr int kStage = kDepth + 1;        // staging slots
+    constexpr int kRing = 4;                  // population rows
+    constexpr int kPer = 16 / (int)sizeof(T); // cells per 16-byte copy
+    constexpr int kSW = TX + kPer;            // staged cells per row, from xs (see below)
     constexpr int kCopies = kSW / kPer;       // 16-byte copies per staged moment row
-    static_assert(TX % kPer == 0, "strips start on copy boundaries");
+    static_assert(TX % kPer == 0, "whole copies per staged row");
     __shared__ __align__(16) T stage[kStage][6][kSW];
-    __shared__ float ring[kRing][9][TX + 2];
+    __shared__ float ring[kRing][9][TX];
 
     const int n = (int)act->n;
     if (n == 0) return;
@@ -173,12 +175,15 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
         const uint32_t local = t - act->tile_prefix[a];
         const uint32_t tw = act->tiles_x[a];
         const GridArgs<T> g = episode_args<T>(eps[act->slot[a]], parity);
-        const int x0 = (int)(local % tw) * TX;
+        const int x0 = (int)(local % tw) * kOut;
         const int yb = (int)(local / tw) * CH, ye = min(yb + CH, g.ny);
         const bool wx = g.periodic & 1, wy = g.periodic & 2;
-        // whole copies start on 16-byte bounds when a row holds a multiple
-        // of P cells (then so does every moment plane, and x0 is a multiple
-        // of P; the buffers themselves are 256-byte aligned)
+        // staged window: cells xs .. xs+kSW-1, xs the copy bound at or below
+        // x0-1 (0 for the first strip), which covers the halo row x0-1 .. x0+TX-2
+        const int xs = (max(x0 - 1, 0) / kPer) * kPer;
+        // whole copies start on 16-byte bounds when a row holds a multiple of
+        // kPer cells (then so does every moment plane; the buffers themselves
+        // are 256-byte aligned)
         const bool vec = g.nx % kPer == 0;
         // stage row r (yb-1 <= r <= ye): the cells that lie inside the grid
         auto issue = [&](int r) {
@@ -188,26 +193,24 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
                 if (vec) {
                     for (int e = tid; e < 6 * kCopies; e += TX) {
                         const int k = e / kCopies, w = e - k * kCopies;
-                        const int x = x0 - kPer + w * kPer;
-                        if (x >= 0 && x + kPer <= g.nx)
-                            cp_async16(&st[k][w * kPer], g.src + (size_t)k * g.ncell + row + x);
+                        const int x = xs + w * kPer;
+                        if (x + kPer <= g.nx) cp_async16(&st[k][w * kPer], g.src + (size_t)k * g.ncell + row + x);
                     }
                 } else {
                     for (int e = tid; e < 6 * kSW; e += TX) {
                         const int k = e / kSW, j = e - k * kSW;
-                        const int x = x0 - kPer + j;
-                        if (x >= 0 && x < g.nx) st[k][j] = g.src[(size_t)k * g.ncell + row + x];
+                        if (xs + j < g.nx) st[k][j] = g.src[(size_t)k * g.ncell + row + xs + j];
                     }
                 }
             }
             cp_async_commit();
         };
-        // reconstruct halo column c (cell x0-1+c) of row r into the ring; the
-        // clamped or wrapped source column is read from the staged row when it
-        // lies there, else (a wrapped edge) from memory
-        auto recon = [&](int r, int c) {
-            const int gx = halo_index(x0 - 1 + c, g.nx, wx);
-            const int j = gx - (x0 - kPer);
+        // reconstruct this thread's halo cell x0-1+tid of row r into the
+        // ring; the clamped or wrapped source column is read from the staged
+        // row when it lies there, else (a wrapped edge) from memory
+        auto recon = [&](int r) {
+            const int gx = halo_index(x0 - 1 + tid, g.nx, wx);
+            const int j = gx - xs;
             T raw[6];
             if (j >= 0 && j < kSW) {
                 const T (*st)[kSW] = stage[(r + kStage) % kStage];
@@ -220,33 +223,30 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
             }
             float f[9];
             dense2d_recon<T, false>(g, raw, f);
-            float (*rg)[TX + 2] = ring[(r + kRing) % kRing];
+            float (*rg)[TX] = ring[(r + kRing) % kRing];
 #pragma unroll
-            for (int i = 0; i < 9; ++i) rg[i][c] = f[i];
+            for (int i = 0; i < 9; ++i) rg[i][tid] = f[i];
         };
 
 #pragma unroll
         for (int r = 0; r < kDepth; ++r) issue(yb - 1 + r);
-        const int x = x0 + tid;
+        const int x = x0 - 1 + tid;
+        const bool owner = tid >= 1 && tid <= kOut && x < g.nx; // this thread updates column x
         uint32_t f8 = 0; // flag byte of the next output row's cell
         for (int r = yb - 1; r <= ye + 1; ++r) {
             cp_async_wait<kDepth - 1>(); // this thread's copies of row r have landed
             __syncthreads();             // everyone's copies of row r, and ring row r-1, are visible
             issue(r + kDepth);           // into the slot of row r-1, reconstructed last iteration
-            if (r <= ye) {
-                recon(r, tid + 1);
-                if (tid == 0) recon(r, 0);
-                if (tid == TX - 1) recon(r, TX + 1);
-            }
+            if (r <= ye) recon(r);
             // output row o: its ring rows o-1, o, o+1 were written before the barrier
             const int o = r - 2;
-            if (o >= yb && x < g.nx && is_updated(f8 & kTypeMask) && !(f8 & kBitLink)) {
+            if (o >= yb && owner && is_updated(f8 & kTypeMask) && !(f8 & kBitLink)) {
                 const uint32_t idx = (uint32_t)(o * g.nx + x);
                 dense2d_update_cell(
-                    g, idx, f8, [&](int i) { return ring[(o - L::cy(i) + kRing) % kRing][i][tid + 1 - L::cx(i)]; },
-                    [&](int i) { return ring[(o + kRing) % kRing][i][tid + 1]; });
+                    g, idx, f8, [&](int i) { return ring[(o - L::cy(i) + kRing) % kRing][i][tid - L::cx(i)]; },
+                    [&](int i) { return ring[(o + kRing) % kRing][i][tid]; });
             }
-            f8 = (o + 1 >= yb && o + 1 < ye && x < g.nx) ? (uint32_t)g.flags[(size_t)(o + 1) * g.nx + x] : 0u;
+            f8 = (owner && o + 1 >= yb && o + 1 < ye) ? (uint32_t)g.flags[(size_t)(o + 1) * g.nx + x] : 0u;
         }
     }
 }

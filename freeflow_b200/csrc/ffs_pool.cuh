@@ -99,15 +99,15 @@ __host__ __device__ inline void swimmer_vertex(float rx, float ry, float amp, fl
 
 // Work units of the batched dense pass (the autotuner's candidates): tiles
 // of tx x ty cells, one thread per cell (pool_dense_kernel), or strips of tx
-// columns and ty rows walked row by row by tx threads (pool_strip_kernel).
+// columns and ty rows walked row by row by tx + 2 threads (pool_strip_kernel).
 struct PoolTileShape {
     int tx, ty;
     bool strip;
 };
 constexpr int kPoolNumShapes = 8;
 constexpr PoolTileShape kPoolShapes[kPoolNumShapes] = {{32, 4, false},  {32, 8, false},  {64, 4, false},
-                                                       {32, 16, false}, {64, 8, false},  {64, 32, true},
-                                                       {128, 32, true}, {128, 64, true}};
+                                                       {32, 16, false}, {64, 8, false},  {62, 32, true},
+                                                       {126, 32, true}, {126, 64, true}};
 
 cudaError_t launch_pool_kinematics(const PoolEpisode *eps, const PoolParams *prm, const PoolActive *act, int substep,
                                    int grid, cudaStream_t st);
