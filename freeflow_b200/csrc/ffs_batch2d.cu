@@ -232,7 +232,13 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
         for (int r = 0; r < kDepth; ++r) issue(yb - 1 + r);
         const int x = x0 - 1 + tid;
         const bool owner = tid >= 1 && tid <= kOut && x < g.nx; // this thread updates column x
-        uint32_t f8 = 0; // flag byte of the next output row's cell
+        // flag bytes of this thread's cell: at the top of iteration r, f8 is
+        // that of row r-2 (updated this iteration) and f8n that of row r-1;
+        // row r's is loaded at the end of iteration r, two iterations ahead
+        auto flag_at = [&](int y) -> uint32_t {
+            return (owner && y >= yb && y < ye) ? (uint32_t)g.flags[(size_t)y * g.nx + x] : 0u;
+        };
+        uint32_t f8 = 0, f8n = 0;
         for (int r = yb - 1; r <= ye + 1; ++r) {
             cp_async_wait<kDepth - 1>(); // this thread's copies of row r have landed
             __syncthreads();             // everyone's copies of row r, and ring row r-1, are visible
@@ -246,7 +252,8 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
                     g, idx, f8, [&](int i) { return ring[(o - L::cy(i) + kRing) % kRing][i][tid - L::cx(i)]; },
                     [&](int i) { return ring[(o + kRing) % kRing][i][tid]; });
             }
-            f8 = (owner && o + 1 >= yb && o + 1 < ye) ? (uint32_t)g.flags[(size_t)(o + 1) * g.nx + x] : 0u;
+            f8 = f8n;
+            f8n = flag_at(o + 2);
         }
     }
 }
