@@ -41,6 +41,7 @@ struct ffs_lbm {
     Codec codec{};
     LinkTable lt;
     float *staging = nullptr; // ncell * NM floats, allocated on first host transfer
+    uint32_t *fill_bits = nullptr; // D3Q27 solid fill: one parity bit per cell, zero between calls
     int dense_variant = -1;   // D3Q27 kernel variant chosen on the first step (tune_dense3d)
     // link detection runs on `side` while the dense pass runs on the caller's
     // stream; fork/join order them
@@ -432,6 +433,7 @@ ffs_status ffs_lbm_destroy(ffs_lbm *h)
     if (h->side) cudaStreamDestroy(h->side);
     cudaFree(h->mom[0]); cudaFree(h->mom[1]); cudaFree(h->flags); cudaFree(h->wallmask); cudaFree(h->status);
     cudaFree(h->staging);
+    cudaFree(h->fill_bits);
     free_links(h->lt);
     delete h;
     return FFS_OK;
@@ -551,11 +553,19 @@ ffs_status ffs_lbm_step(ffs_lbm *h, const ffs_surface *s, void *stream)
 ffs_status ffs_lbm_fill_solid(ffs_lbm *h, const ffs_surface *s, void *stream)
 {
     if (!h || !s) return fail(FFS_ERR_INVALID_ARGUMENT, "null argument");
-    if (h->dim != 2) return fail(FFS_ERR_UNSUPPORTED, "fill_solid is defined for 2D grids (fillSolidFlags2D)");
     ffs_status r = check_surface(h, s);
     if (r != FFS_OK) return r;
     cudaStream_t st = S(stream);
-    FFS_CK(launch_fill_solid2(h->flags, h->d.nx, h->d.ny, h->cl, surface_args(s), st));
+    if (h->dim == 2) {
+        FFS_CK(launch_fill_solid2(h->flags, h->d.nx, h->d.ny, h->cl, surface_args(s), st));
+    } else {
+        if (!h->fill_bits) {
+            const size_t bytes = sizeof(uint32_t) * (size_t)h->d.ny * h->d.nz * ((h->d.nx + 31) / 32);
+            FFS_CK(cudaMalloc(&h->fill_bits, bytes));
+            FFS_CK(cudaMemsetAsync(h->fill_bits, 0, bytes, st));
+        }
+        FFS_CK(launch_fill_solid3(h->flags, h->fill_bits, h->d.nx, h->d.ny, h->d.nz, h->cl, surface_args(s), st));
+    }
     return prepare_flags(h, st);
 }
 

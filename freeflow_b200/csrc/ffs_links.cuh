@@ -55,6 +55,9 @@ cudaError_t launch_prepare_flags(uint8_t *flags, uint32_t *wallmask, int nx, int
 template <int DIM, typename T>
 cudaError_t launch_initialize(const GridArgs<T> &g, T *other, const float *bcvel, cudaStream_t st);
 cudaError_t launch_fill_solid2(uint8_t *flags, int nx, int ny, float cl, const SurfaceArgs &s, cudaStream_t st);
+// bits: ny * nz * ceil(nx / 32) words, zero on entry and on return
+cudaError_t launch_fill_solid3(uint8_t *flags, uint32_t *bits, int nx, int ny, int nz, float cl, const SurfaceArgs &s,
+                               cudaStream_t st);
 
 template <int DIM, typename T>
 cudaError_t launch_convert_in(const float *in, bool aos, T *out, uint32_t ncell, Codec c, cudaStream_t st);

@@ -160,7 +160,12 @@ ffs_status ffs_lbm_step_noalloc(ffs_lbm *grid, const ffs_surface *surface, void 
 
 /* fsi_coupling::fillSolidFlags2D (FsiCoupling2D.cu:434-464): Fluid cells
  * whose centre lies inside the closed polygon become SolidDynamic, and
- * SolidDynamic cells outside it return to Fluid.  dim == 2 only. */
+ * SolidDynamic cells outside it return to Fluid.  On a D3Q27 grid the same
+ * for a closed triangle mesh, by the parity of the triangles that a ray from
+ * the cell centre along +x crosses: the 3D inside test of the reference
+ * (SolidGeometryProxy_Device<3>::isInside, SolidGeometryProxy_Device.cuh:
+ * 231-289, which has no fill of its own), evaluated row by row.  Elements
+ * with a vertex index out of range are skipped. */
 ffs_status ffs_lbm_fill_solid(ffs_lbm *grid, const ffs_surface *surface, void *stream);
 
 /* Reads (and optionally clears) the device status word; synchronises

@@ -105,6 +105,153 @@ static geo_hit geo_isect3(const float *V, const uint32_t *E, int e, const float 
     return r;
 }
 
+/* ---------------------------------------------------------- 3D solid fill
+ * The reference defines a 3D inside test, SolidGeometryProxy_Device<3>::
+ * isInside (SolidGeometryProxy_Device.cuh:231-289: parity of the triangles
+ * that the segment from the point to the origin crosses, with the
+ * NumericUtils tolerances), but no 3D counterpart of fillSolidFlags2D.
+ *
+ * ffo_inside3_ref restates that test for one point.  ffo_fill_solid3 is the
+ * product's 3D fill (ffs_lbm_fill_solid on a D3Q27 grid), restated with the
+ * same float operations in the same order, so the two give the same flags:
+ *   - rays run along +x through the (y, z) rows of cell centres;
+ *   - a triangle is crossed by the row at (qy, qz) when the point lies in its
+ *     (y, z) projection, by edge functions evaluated in vertex-index order
+ *     (two triangles sharing an edge see exactly opposite values) with ties
+ *     given to edges that point up in y (then z), so a row through a shared
+ *     edge or vertex is counted once per sheet;
+ *   - the crossing's x comes from the edge functions as barycentric weights,
+ *     and it toggles the parity of every cell centre to its left;
+ *   - Fluid and SolidDynamic cells become SolidDynamic where the parity is
+ *     odd and Fluid elsewhere, like resetSolidFlagKernel +
+ *     updateSolidFlagKernel (FsiCoupling2D.cu:318-354) in 2D. */
+static float fs3_edge(const float *p, const float *s, float qy, float qz)
+{
+    return (s[1] - p[1]) * (qz - p[2]) - (s[2] - p[2]) * (qy - p[1]);
+}
+
+static float fs3_dir(const float *V, uint32_t iu, uint32_t iv, float qy, float qz, int *tie)
+{
+    const float *u = V + 3 * (size_t)iu, *v = V + 3 * (size_t)iv;
+    *tie = (v[1] > u[1]) || (v[1] == u[1] && v[2] > u[2]);
+    return iu < iv ? fs3_edge(u, v, qy, qz) : -fs3_edge(v, u, qy, qz);
+}
+
+static int fs3_incl(float e, int tie) { return e > 0.0f || (e == 0.0f && tie); }
+
+static int fs3_cross(const float *V, uint32_t ia, uint32_t ib, uint32_t ic, float qy, float qz, float *xc)
+{
+    int t0, t1, t2;
+    const float e0 = fs3_dir(V, ib, ic, qy, qz, &t0);
+    const float e1 = fs3_dir(V, ic, ia, qy, qz, &t1);
+    const float e2 = fs3_dir(V, ia, ib, qy, qz, &t2);
+    if (e0 == 0.0f && e1 == 0.0f && e2 == 0.0f) return 0;
+    const int pos = fs3_incl(e0, t0) && fs3_incl(e1, t1) && fs3_incl(e2, t2);
+    const int neg = fs3_incl(-e0, !t0) && fs3_incl(-e1, !t1) && fs3_incl(-e2, !t2);
+    if (!pos && !neg) return 0;
+    const float ax = V[3 * (size_t)ia], bx = V[3 * (size_t)ib], cx = V[3 * (size_t)ic];
+    *xc = ((e0 * ax + e1 * bx) + e2 * cx) / ((e0 + e1) + e2);
+    return 1;
+}
+
+/* cells x in [0, nx) whose centre ((x + 0.5) cl) lies left of xc */
+static int fs3_count_left(float xc, float cl, int nx)
+{
+    if (xc != xc) return 0;
+    const float t = xc / cl - 0.5f;
+    int k = !(t > 0.0f) ? 0 : (t >= (float)nx ? nx : (int)ceilf(t));
+    while (k > 0 && ((float)(k - 1) + 0.5f) * cl >= xc) --k;
+    while (k < nx && ((float)k + 0.5f) * cl < xc) ++k;
+    return k;
+}
+
+/* first and last row index (clamped to [0, n)) whose centre can lie in
+ * [lo, hi], padded by one row on each side */
+static void fs3_rows(float lo, float hi, float cl, int n, int *r0, int *r1)
+{
+    float a = floorf(lo / cl - 0.5f) - 1.0f, b = ceilf(hi / cl - 0.5f) + 1.0f;
+    a = fminf(fmaxf(a, 0.0f), (float)n);
+    b = fminf(fmaxf(b, -1.0f), (float)(n - 1));
+    *r0 = (int)a;
+    *r1 = (int)b;
+}
+
+void ffo_fill_solid3(uint8_t *flags, int nx, int ny, int nz, float cl, const float *V, int nv, const uint32_t *E, int ne)
+{
+    const int words = (nx + 31) / 32;
+    const size_t rows = (size_t)ny * nz;
+    uint32_t *bits = (uint32_t *)calloc(rows * words, sizeof(uint32_t));
+    if (!bits) return;
+    for (int i = 0; i < ne; ++i) {
+        const uint32_t ia = E[3 * (size_t)i], ib = E[3 * (size_t)i + 1], ic = E[3 * (size_t)i + 2];
+        if (ia >= (uint32_t)nv || ib >= (uint32_t)nv || ic >= (uint32_t)nv) continue;
+        int finite = 1;
+        for (int k = 0; k < 3; ++k)
+            finite &= isfinite(V[3 * (size_t)ia + k]) && isfinite(V[3 * (size_t)ib + k]) && isfinite(V[3 * (size_t)ic + k]);
+        if (!finite) continue;
+        const float *a = V + 3 * (size_t)ia, *b = V + 3 * (size_t)ib, *c = V + 3 * (size_t)ic;
+        int y0, y1, z0, z1;
+        fs3_rows(fminf(fminf(a[1], b[1]), c[1]), fmaxf(fmaxf(a[1], b[1]), c[1]), cl, ny, &y0, &y1);
+        fs3_rows(fminf(fminf(a[2], b[2]), c[2]), fmaxf(fmaxf(a[2], b[2]), c[2]), cl, nz, &z0, &z1);
+        for (int z = z0; z <= z1; ++z)
+            for (int y = y0; y <= y1; ++y) {
+                const float qy = ((float)y + 0.5f) * cl, qz = ((float)z + 0.5f) * cl;
+                float xc;
+                if (!fs3_cross(V, ia, ib, ic, qy, qz, &xc)) continue;
+                const int k = fs3_count_left(xc, cl, nx);
+                if (k < 1) continue;
+                bits[((size_t)z * ny + y) * words + (size_t)((k - 1) >> 5)] ^= 1u << ((k - 1) & 31);
+            }
+    }
+    for (size_t r = 0; r < rows; ++r) {
+        uint32_t par = 0;
+        for (int x = nx - 1; x >= 0; --x) {
+            par ^= (bits[r * words + (size_t)(x >> 5)] >> (x & 31)) & 1u;
+            uint8_t *f = flags + r * nx + x;
+            if (*f == FL_FLUID || *f == FL_SOLIDDYN) *f = par ? FL_SOLIDDYN : FL_FLUID;
+        }
+    }
+    free(bits);
+}
+
+/* SolidGeometryProxy_Device<3>::isInside (SolidGeometryProxy_Device.cuh:231-289) */
+int ffo_inside3_ref(const float *V, const uint32_t *E, int ne, float px, float py, float pz)
+{
+    const float eps = 1e-6f;
+    const float p[3] = {px, py, pz};
+    int inside = 0;
+    for (int i = 0; i < ne; ++i) {
+        float v[3][3];
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) v[j][k] = V[(size_t)E[3 * (size_t)i + j] * 3 + k];
+        float e1[3], e2[3], n[3], d[3];
+        for (int k = 0; k < 3; ++k) { e1[k] = v[1][k] - v[0][k]; e2[k] = v[2][k] - v[0][k]; d[k] = p[k]; }
+        geo_cross(e1, e2, n);
+        geo_normalize(d);
+        if (fabsf(geo_dot(n, d)) <= 0.0f + eps) continue;
+        float w0[3], op[3];
+        for (int k = 0; k < 3; ++k) { w0[k] = v[0][k] - p[k]; op[k] = -p[k]; }
+        const float t = geo_dot(n, w0) / geo_dot(n, op);
+        if (t <= 0.0f + eps || t > 1.0f + eps) continue;
+        float hit[3];
+        for (int k = 0; k < 3; ++k) hit[k] = p[k] + t * op[k];
+        int same = 1;
+        for (int j = 0; j < 3 && same; ++j) {
+            const float *a = v[j], *b = v[(j + 1) % 3], *c = v[(j + 2) % 3];
+            float ba[3], ca[3], ha[3], c1[3], c2[3];
+            for (int k = 0; k < 3; ++k) { ba[k] = b[k] - a[k]; ca[k] = c[k] - a[k]; ha[k] = hit[k] - a[k]; }
+            geo_cross(ba, ca, c1);
+            const float vn = sqrtf(geo_dot(c1, c1));
+            for (int k = 0; k < 3; ++k) c1[k] = c1[k] / vn;
+            geo_cross(ba, ha, c2);
+            for (int k = 0; k < 3; ++k) c2[k] = c2[k] / vn;
+            if (geo_dot(c1, c2) <= 0.0f + eps) same = 0;
+        }
+        if (same) inside = !inside;
+    }
+    return inside;
+}
+
 #define R float
 #define FN(x) ffo32_##x
 #include "ffs_oracle_impl.h"

@@ -65,6 +65,9 @@ def lib():
         getattr(L, pre + "reconstruct_at").restype = f64
         getattr(L, pre + "reconstruct_at").argtypes = [i32, vp, i32]
         getattr(L, pre + "collide_pops").argtypes = [i32, vp, f64, vp]
+    L.ffo_fill_solid3.argtypes = [vp, i32, i32, i32, C.c_float, vp, i32, vp, i32]
+    L.ffo_inside3_ref.restype = i32
+    L.ffo_inside3_ref.argtypes = [vp, vp, i32, C.c_float, C.c_float, C.c_float]
     L.ffo_set_threads.argtypes = [i32]
     L.ffo_get_threads.restype = i32
     L.ffo_round_half.restype = C.c_float
@@ -106,6 +109,24 @@ def collide_pops(dim: int, pops, omega: float, precision="phys64") -> np.ndarray
     pre = "ffo32_" if precision == "ref32" else "ffo64_"
     getattr(lib(), pre + "collide_pops")(dim, _ptr(p), float(omega), _ptr(out))
     return out
+
+
+def fill_solid3(flags, nx: int, ny: int, nz: int, cl: float, vertices, elements) -> np.ndarray:
+    """The product's D3Q27 solid fill restated (ffo_fill_solid3): returns the
+    new flag array; Fluid/SolidDynamic cells inside the closed triangle mesh
+    become SolidDynamic, the others Fluid; every other flag is kept."""
+    f = np.array(flags, dtype=np.uint8, copy=True).reshape(-1)
+    V = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1)
+    E = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1)
+    lib().ffo_fill_solid3(_ptr(f), nx, ny, nz, float(cl), _ptr(V), V.size // 3, _ptr(E), E.size // 3)
+    return f
+
+
+def inside3_ref(vertices, elements, p) -> bool:
+    """The reference's SolidGeometryProxy_Device<3>::isInside for one point."""
+    V = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1)
+    E = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1)
+    return bool(lib().ffo_inside3_ref(_ptr(V), _ptr(E), E.size // 3, float(p[0]), float(p[1]), float(p[2])))
 
 
 class Oracle:
