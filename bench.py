@@ -17,6 +17,16 @@ the max over ranks and value = all cells updated / that time ("weak").
 ``--impl reference`` times the reference's algorithm on the host cores: the
 FP32 restatement in oracle/ (the reference's CUDA sources do not build here)
 with all host threads, each step a z-slab sample of the same workload.
+
+The default line (N = 1) also carries:
+  storage                 config D with FP16 and BF16 moment storage (GPU);
+  serving                 config E, the batched FP16 pool against the plain
+                          per-episode FP32 path (GPU);
+  cpu_baseline and        the CPU leg, the only part of the GPU arm that runs
+  storage_errors_vs_fp64  the oracle: its FP32 restatement timed on the host
+                          cores, and its FP64 build as the checker of the
+                          reduced-storage GPU results (skipped with
+                          --no-cpu-baseline).
 """
 from __future__ import annotations
 
@@ -220,6 +230,91 @@ def oracle_slab_run(wl: W.Workload, steps: int, warmup: int, nz_slab: int, threa
     return cells * steps / dt / 1e6, cells, dt
 
 
+def serving_velocity_error(storage: str, control_steps: int = 20, sides: str = "walls"):
+    """Relative L2 velocity error of a pool episode (256x128 swimmer) against
+    the FP64 oracle run on the same surfaces, after `control_steps` x 10 substeps."""
+    from freeflow_b200 import serving as S
+    from oracle.oracle import Oracle
+
+    sp = S.make_episode(256, 128, seed=51, length=control_steps, sides=sides)
+    pool = S.Pool(storage=storage, budget_bytes=256 << 20, max_episodes=2)
+    slot = pool.admit(sp)
+    o = Oracle(2, sp.nx, sp.ny, 1, viscosity=sp.viscosity, density=sp.density, dx=sp.dx, dt=sp.dt,
+               boundary_velocities=[0, 0, 0, 0], periodic=0, precision="phys64")
+    o.set_flags(sp.flags)
+    o.set_moments(pool.get_moments(slot).astype(np.float64))
+    q = 0
+    for c in range(control_steps):
+        a = np.random.default_rng(c).uniform(-1, 1, 8).astype(np.float32)
+        pool.set_action(slot, a)
+        pool.advance()
+        for _ in range(pool.substeps):
+            V, U = S.swimmer_surface(sp, a, q)
+            o.step(V, U, sp.elements, None)
+            q += 1
+    g = pool.get_moments(slot).astype(np.float64)
+    ref = o.get_moments()
+    err = float(np.linalg.norm(g[:, 1:3] - ref[:, 1:3]) / np.linalg.norm(ref[:, 1:3]))
+    o.close()
+    pool.close()
+    return err
+
+
+def tgv_velocity_errors(storages=("f32", "f16", "bf16"), n: int = 48, steps: int = 100):
+    """Relative L2 velocity error of a D3Q27 periodic Taylor-Green vortex (n^3,
+    peak velocity 0.04, viscosity 0.005) after `steps` steps on the GPU with
+    each moment storage, against one run of the oracle's FP64 build."""
+    from freeflow_b200 import FluidGrid
+    from oracle.oracle import Oracle
+
+    wl = W.taylor_green_3d(n=n, u0=0.04, viscosity=0.005)
+    o = Oracle(3, n, n, n, viscosity=wl.fluid_viscosity, density=wl.fluid_density, dx=wl.fluid_dx, dt=wl.dt,
+               boundary_velocities=wl.boundary_velocities, periodic=wl.periodic, precision="phys64")
+    o.set_flags(wl.flags)
+    o.set_moments(wl.moments.astype(np.float64))
+    for _ in range(steps):
+        o.step()
+    ref = o.get_moments()[:, 1:4]
+    o.close()
+    out = {}
+    for st in storages:
+        g = FluidGrid(**wl.grid_kwargs(storage=st))
+        g.set_flags(wl.flags)
+        g.set_moments(wl.moments)
+        for _ in range(steps):
+            g.step()
+        got = g.get_moments().astype(np.float64)[:, 1:4]
+        g.close()
+        out[st] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    return out
+
+
+def cpu_leg(wl: W.Workload, threads: int):
+    """The CPU leg of the GPU arm, the one place where this arm runs the oracle:
+    the oracle's FP32 restatement timed on the host cores (the CPU baseline, a
+    z-slab sample of about 20 s of CPU work), and the oracle's FP64 build as
+    the checker of the reduced-storage GPU outputs.  Returns (cpu_baseline,
+    errors against FP64)."""
+    rate = 4.0e6 * threads / 8.0
+    nz_slab = int(20.0 * rate / 3 / (wl.nx * wl.ny)) if wl.dim == 3 else 1
+    mlups, cells, sec = oracle_slab_run(wl, 3, 1, nz_slab, threads)
+    cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+           "sample": (f"3 steps of a {cells // (wl.nx * wl.ny)}-plane z-slab of {wl.name}" if wl.dim == 3
+                      else f"3 steps of {wl.name}") + f", FP32 restatement, {sec:.1f} s"}
+    errors = {
+        "serving_2d": {
+            "closed_tank": {"f16": serving_velocity_error("f16"), "f32": serving_velocity_error("f32")},
+            "outlets": {"f16": serving_velocity_error("f16", sides="outlets"),
+                        "f32": serving_velocity_error("f32", sides="outlets")},
+            "case": "pool episode, 256x128 swimmer, 200 substeps, same surfaces as the FP64 oracle; with outlets "
+                    "the reference's sign-switched outlet rule makes even FP32 differ from FP64 (branch flips)"},
+        "taylor_green_3d": tgv_velocity_errors(),
+        "taylor_green_3d_case": "D3Q27 periodic 48^3, u0 0.04, viscosity 0.005, 100 steps, relative L2 of u",
+        "target": "f16 relative velocity error <= 1e-3",
+    }
+    return cpu, errors
+
+
 def run_reference(args):
     from freeflow_b200 import replicas as R
 
@@ -251,36 +346,6 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- serving
-def serving_velocity_error(storage: str, control_steps: int = 20, sides: str = "walls"):
-    """Relative L2 velocity error of a pool episode (256x128 swimmer) against
-    the FP64 oracle run on the same surfaces, after `control_steps` x 10 substeps."""
-    from freeflow_b200 import serving as S
-    from oracle.oracle import Oracle
-
-    sp = S.make_episode(256, 128, seed=51, length=control_steps, sides=sides)
-    pool = S.Pool(storage=storage, budget_bytes=256 << 20, max_episodes=2)
-    slot = pool.admit(sp)
-    o = Oracle(2, sp.nx, sp.ny, 1, viscosity=sp.viscosity, density=sp.density, dx=sp.dx, dt=sp.dt,
-               boundary_velocities=[0, 0, 0, 0], periodic=0, precision="phys64")
-    o.set_flags(sp.flags)
-    o.set_moments(pool.get_moments(slot).astype(np.float64))
-    q = 0
-    for c in range(control_steps):
-        a = np.random.default_rng(c).uniform(-1, 1, 8).astype(np.float32)
-        pool.set_action(slot, a)
-        pool.advance()
-        for _ in range(pool.substeps):
-            V, U = S.swimmer_surface(sp, a, q)
-            o.step(V, U, sp.elements, None)
-            q += 1
-    g = pool.get_moments(slot).astype(np.float64)
-    ref = o.get_moments()
-    err = float(np.linalg.norm(g[:, 1:3] - ref[:, 1:3]) / np.linalg.norm(ref[:, 1:3]))
-    o.close()
-    pool.close()
-    return err
-
-
 def run_serving(iterations: int, warmup: int, concurrency: int = 256, plain_steps: int = 20, seed: int = 0):
     """Config E: Poisson stream of 2D swimmer episodes (grids uniform over
     256x128, 512x192, 1200x400; 8 actions per control step; 10 substeps per
@@ -318,15 +383,58 @@ def run_serving(iterations: int, warmup: int, concurrency: int = 256, plain_step
                  "dense_roofline": ({"achieved": round(dense_gbs, 1), "peak": peak, "unit": "GB/s",
                                      "frac": round(dense_gbs / peak, 4), "bytes_per_cell": 25,
                                      "peak_kind": peak_kind} if dense_gbs else None)},
-        "velocity_rel_err_vs_fp64": {
-            "closed_tank": {"f16": serving_velocity_error("f16"), "f32": serving_velocity_error("f32")},
-            "outlets": {"f16": serving_velocity_error("f16", sides="outlets"),
-                        "f32": serving_velocity_error("f32", sides="outlets")},
-            "case": "256x128 swimmer, 200 substeps, same surfaces as the FP64 oracle; with outlets the "
-                    "reference's sign-switched outlet rule makes even FP32 differ from FP64 (branch flips)"},
         "seconds": round(time.perf_counter() - t0, 1),
     }
     return out
+
+
+def run_storage_d(wl: W.Workload, storage: str, steps: int = 40, warmup: int = 5):
+    """Config D with reduced moment storage (scaled deviations, FP32 compute):
+    whole-step MLUPS and the dense kernel's time and bandwidth, device-resident
+    surfaces, CUDA events."""
+    import torch
+    from freeflow_b200 import DeviceSurface, FluidGrid
+
+    g = FluidGrid(**wl.grid_kwargs(storage=storage))
+    g.set_flags(wl.flags)
+    g.set_moments(wl.moments)
+    v0, u0 = wl.surface_at(0)
+    surf = DeviceSurface(v0, u0, wl.elements)
+    g.reserve_surface(surf.num_vertices, max(4096, surf.num_elements * 40))
+    Vd = torch.from_numpy(np.stack([wl.surface_at(s)[0] for s in range(steps + warmup)])).cuda()
+    Ud = torch.from_numpy(np.stack([wl.surface_at(s)[1] for s in range(steps + warmup)])).cuda()
+    stream = torch.cuda.Stream()
+
+    def step(s):
+        surf.vertices, surf.velocities = Vd[s], Ud[s]
+        g.step(surf, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for s in range(warmup):
+            step(s)
+    torch.cuda.synchronize()
+    g.profile(True)
+    g.profile_read(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for s in range(steps):
+            step(warmup + s)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    g.profile(False)
+    prof = g.profile_read(reset=True)
+    ms = e0.elapsed_time(e1)
+    status = g.status(clear=True)
+    g.close()
+    peak, peak_kind = hbm_peak()
+    bpc = algorithmic_bytes_per_cell(3, storage)
+    dense_ms = prof["dense"][0] / max(1, prof["dense"][1])
+    return {"mlups": round(wl.ncell * steps / (ms * 1e-3) / 1e6, 1), "ms_per_step": round(ms / steps, 4),
+            "dense_ms": round(dense_ms, 4), "bytes_per_cell": bpc,
+            "dense_gbs": round(wl.ncell * bpc / (dense_ms * 1e-3) / 1e9, 1),
+            "dense_frac": round(wl.ncell * bpc / (dense_ms * 1e-3) / 1e9 / peak, 4), "peak_kind": peak_kind,
+            "device_status": status}
 
 
 def run_serving_line(args):
@@ -475,15 +583,9 @@ def run_ours(args):
     traffic_src = f"{tpc[0]} B/cell measured by ncu, scaled to {wl.ncell} cells ({tpc[1]})" if tpc else None
     out = None
     if rank == 0:
-        cpu = None
+        cpu, errors = None, None
         if world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            rate = 4.0e6 * threads / 8.0
-            nz_slab = int(20.0 * rate / 3 / (wl.nx * wl.ny)) if wl.dim == 3 else 1
-            mlups, cells, sec = oracle_slab_run(wl, 3, 1, nz_slab, threads)
-            cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-                   "sample": (f"3 steps of a {cells // (wl.nx * wl.ny)}-plane z-slab of {wl.name}" if wl.dim == 3
-                              else f"3 steps of {wl.name}") + f", FP32 restatement, {sec:.1f} s"}
+            cpu, errors = cpu_leg(wl, os.cpu_count() or 1)
         out = {
             "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
             "warmup": Wm, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
@@ -505,6 +607,10 @@ def run_ours(args):
             "clocks": clk,
             "device_status": status,
         }
+        if errors is not None:
+            out["storage_errors_vs_fp64"] = errors
+        if world == 1 and not args.small and args.workload == "D" and storage == "f32":
+            out["storage"] = {st: run_storage_d(wl, st) for st in ("f16", "bf16")}
         if world == 1 and not args.no_serving and not args.small:
             out["serving"] = run_serving(iterations=150, warmup=20)
         print(json.dumps(out), flush=True)
