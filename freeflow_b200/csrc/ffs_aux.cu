@@ -60,7 +60,7 @@ template <int DIM>
 cudaError_t launch_prepare_flags(uint8_t *flags, uint32_t *wallmask, int nx, int ny, int nz, cudaStream_t st)
 {
     long long n = (long long)nx * ny * nz;
-    int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    int grid = (int)std::min<long long>((n + 255) / 256, (long long)device_sms() * 16);
     prepare_flags_kernel<DIM><<<grid, 256, 0, st>>>(flags, wallmask, nx, ny, nz);
     return cudaGetLastError();
 }
@@ -107,7 +107,7 @@ cudaError_t launch_initialize(const GridArgs<T> &g, T *other, const float *bcvel
 {
     Vel6 bc;
     for (int i = 0; i < 6; ++i) bc.v[i] = bcvel[i];
-    int grid = (int)std::min<long long>(((long long)g.ncell + 255) / 256, 148LL * 16);
+    int grid = (int)std::min<long long>(((long long)g.ncell + 255) / 256, (long long)device_sms() * 16);
     initialize_kernel<DIM, T><<<grid, 256, 0, st>>>(g, other, bc);
     return cudaGetLastError();
 }
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) fill_solid2_kernel(uint8_t *flags, int nx
 
 cudaError_t launch_fill_solid2(uint8_t *flags, int nx, int ny, float cl, const SurfaceArgs &s, cudaStream_t st)
 {
-    const int grid = std::max(1, std::min((ny + 7) / 8, 148 * 8));
+    const int grid = std::max(1, std::min((ny + 7) / 8, device_sms() * 8));
     fill_solid2_kernel<<<grid, 256, 0, st>>>(flags, nx, ny, cl, s);
     return cudaGetLastError();
 }
@@ -320,9 +320,7 @@ __global__ void __launch_bounds__(256) fill_solid3_apply_kernel(uint8_t *flags, 
 cudaError_t launch_fill_solid3(uint8_t *flags, uint32_t *bits, int nx, int ny, int nz, float cl, const SurfaceArgs &s,
                                cudaStream_t st)
 {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = device_sms();
     const int words = (nx + 31) / 32;
     if (s.ne > 0) {
         const int grid = (int)std::max<long long>(1, std::min<long long>((s.ne + 7) / 8, (long long)sms * 16));
@@ -365,14 +363,14 @@ __global__ void convert_out_kernel(const T *in, float *out, bool aos, uint32_t n
 template <int DIM, typename T>
 cudaError_t launch_convert_in(const float *in, bool aos, T *out, uint32_t ncell, Codec c, cudaStream_t st)
 {
-    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, 148LL * 16);
+    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, (long long)device_sms() * 16);
     convert_in_kernel<DIM, T><<<grid, 256, 0, st>>>(in, aos, out, ncell, c);
     return cudaGetLastError();
 }
 template <int DIM, typename T>
 cudaError_t launch_convert_out(const T *in, float *out, bool aos, uint32_t ncell, Codec c, cudaStream_t st)
 {
-    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, 148LL * 16);
+    int grid = (int)std::min<long long>(((long long)ncell + 255) / 256, (long long)device_sms() * 16);
     convert_out_kernel<DIM, T><<<grid, 256, 0, st>>>(in, out, aos, ncell, c);
     return cudaGetLastError();
 }

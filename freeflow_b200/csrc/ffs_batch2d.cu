@@ -4,8 +4,9 @@
 // Work items are numbered across episodes through the prefix sums of the
 // active table (dense tiles, surface elements, surface vertices); an item
 // finds its episode by a binary search over at most kPoolMaxSlots prefixes.
-// The per-item bodies are the single-grid ones (dense2d_tile, detect_pair,
-// link_cell_update), so a pool episode computes bit for bit what the same
+// The per-item bodies are the single-grid ones (dense2d_tile or the same
+// per-cell code in strips, detect_element2_warp, link_cell_update), so a pool
+// episode computes bit for bit what the same
 // grid computes alone through ffs_lbm_step.  The grids are persistent
 // (a fixed number of CTAs striding over a count read from device memory), so
 // one captured CUDA graph serves every mix of episodes.
@@ -90,25 +91,25 @@ __global__ void pool_kinematics_kernel(const PoolEpisode *eps, const PoolParams 
 }
 
 // ---------------------------------------------------------------- detect
+// One warp per element of any episode (the single-grid body,
+// detect_element2_warp); the warp finds the element's episode once.
 template <typename T>
-__global__ void pool_detect_kernel(const PoolEpisode *eps, const PoolActive *act, LinkTable lt, uint32_t *owner,
-                                   int parity)
+__global__ void __launch_bounds__(256) pool_detect_kernel(const PoolEpisode *eps, const PoolActive *act, LinkTable lt,
+                                                          uint32_t *owner, int parity)
 {
     const int n = (int)act->n;
     if (n == 0) return;
-    const long long total = (long long)act->elem_prefix[n] * 8;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total;
-         p += (long long)gridDim.x * blockDim.x) {
-        const uint32_t ge = (uint32_t)(p >> 3);
-        const int l = (int)(p & 7) + 1;
+    const uint32_t total = act->elem_prefix[n];
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t ge = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ge < total; ge += nwarps) {
         const int a = owner_of(act->elem_prefix, n, ge);
         const uint32_t s = act->slot[a];
         const PoolEpisode &e = eps[s];
         const GridArgs<T> g = episode_args<T>(e, parity);
         const SurfaceArgs sa = episode_surface(e);
         const StepScalars sc{e.cl, e.ct, e.cf};
-        detect_pair<2, T>(g, reinterpret_cast<uint32_t *>(e.flags), lt, sa, sc, (long long)(ge - act->elem_prefix[a]),
-                          l, e.cell_base, owner, s);
+        detect_element2_warp<T>(g, reinterpret_cast<uint32_t *>(e.flags), lt, sa, sc,
+                                (long long)(ge - act->elem_prefix[a]), e.cell_base, owner, s);
     }
 }
 
@@ -378,7 +379,7 @@ template <typename T>
 cudaError_t launch_pool_detect(const PoolEpisode *eps, const PoolActive *act, const LinkTable &lt, uint32_t *owner,
                                int parity, int grid, cudaStream_t st)
 {
-    pool_detect_kernel<T><<<grid, 128, 0, st>>>(eps, act, lt, owner, parity);
+    pool_detect_kernel<T><<<grid, 256, 0, st>>>(eps, act, lt, owner, parity);
     return cudaGetLastError();
 }
 

@@ -302,6 +302,15 @@ struct Vel6 {
 
 // --------------------------------------------------------- grid descriptor
 // Everything one fluid grid's kernels need, passed by value.
+// SMs of the current device: grid-stride launches are capped at a multiple of it.
+inline int device_sms()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 1;
+    return n;
+}
+
 // cp.async (LDGSTS): 4-byte global -> shared copies that hold no registers
 // while in flight.  Both addresses must be 4-byte aligned.
 __device__ __forceinline__ void cp_async4(void *dst, const void *src)

@@ -8,7 +8,7 @@
 // (SolidGeometryProxy_Device.cuh:184-194, :401-421).
 //
 // Here the link set is sparse and O(surface):
-//   detect      one thread per (element, direction) tests the cells of the
+//   detect      one warp per element tests the (cell, direction) pairs of the
 //               element's bounding box grown by one cell and inserts hits into
 //               an open-addressing table keyed by cell; per (cell, direction)
 //               atomicMin keeps the nearest (depth, element) key.  The owning
@@ -35,30 +35,17 @@
 namespace fflbm {
 
 // ------------------------------------------------------------------ detect
-static int sm_count()
-{
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+static int sm_count() { return device_sms(); }
 
 // CTAs of `threads` threads of KERNEL that are resident on the device at
-// once (no dynamic shared memory); computed once per kernel.
+// once (no dynamic shared memory); the occupancy is queried once per kernel.
 template <auto KERNEL> static int resident_grid(int threads)
 {
-    static int grid = 0;
-    if (!grid) {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERNEL, threads, 0) != cudaSuccess || per_sm < 1)
-            per_sm = 1;
-        grid = sm_count() * per_sm;
-    }
-    return grid;
+    static int per_sm = 0;
+    if (!per_sm && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERNEL, threads, 0) != cudaSuccess ||
+                    per_sm < 1))
+        per_sm = 1;
+    return sm_count() * per_sm;
 }
 
 // D3Q27: one warp per triangle.  The triangle's own geometry is evaluated
@@ -161,14 +148,14 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
     }
 }
 
-template <int DIM, typename T>
-__global__ void detect_links_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s, StepScalars sc)
+// D2Q9: one warp per segment (detect_element2_warp).
+template <typename T>
+__global__ void __launch_bounds__(256) detect_links2_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt,
+                                                            SurfaceArgs s, StepScalars sc)
 {
-    constexpr int Q = Lattice<DIM>::Q;
-    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long e = gid / (Q - 1);
-    if (e >= s.ne) return;
-    detect_pair<DIM, T>(g, flag_words, lt, s, sc, e, (int)(gid % (Q - 1)) + 1);
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < s.ne; e += nwarps)
+        detect_element2_warp<T>(g, flag_words, lt, s, sc, e);
 }
 
 // -------------------------------------------------------------- link cells
@@ -242,10 +229,8 @@ cudaError_t launch_detect_links(const GridArgs<T> &g, uint32_t *flag_words, cons
         detect_links3_kernel<T><<<grid, 256, 0, st>>>(g, flag_words, lt, s, sc);
         return cudaGetLastError();
     }
-    long long threads = (long long)s.ne * (Q - 1);
-    int block = 128;
-    long long grid = (threads + block - 1) / block;
-    detect_links_kernel<DIM, T><<<(unsigned)grid, block, 0, st>>>(g, flag_words, lt, s, sc);
+    const int grid = (int)std::min<long long>((s.ne + 7) / 8, (long long)sm_count() * 16);
+    detect_links2_kernel<T><<<grid, 256, 0, st>>>(g, flag_words, lt, s, sc);
     return cudaGetLastError();
 }
 

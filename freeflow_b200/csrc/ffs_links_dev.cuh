@@ -56,63 +56,64 @@ __device__ __forceinline__ void insert_link(const LinkTable &lt, uint32_t *flag_
     atomicOr(status, kStatusLinkOverflow);
 }
 
-// Link detection of element e in direction l (1 <= l < Q): every cell of
-// the element's bounding box grown by one cell whose link segment
-// x -> x - c_l crosses the element gets a (depth, element) key.
-template <int DIM, typename T>
-__device__ __forceinline__ void detect_pair(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt,
-                                            const SurfaceArgs &s, const StepScalars &sc, long long e, int l,
-                                            uint32_t key_base = 0, uint32_t *owner = nullptr,
-                                            uint32_t owner_id = 0)
+// D2Q9 link detection of segment e by one warp: every cell of the segment's
+// bounding box grown by one cell (getBoundingBox: min from FLT_MAX, max from
+// FLT_MIN (sic), then / dx) and every direction 1 <= l < 9 whose link segment
+// x -> x - c_l crosses the element gets a (depth, element) key.  Items are
+// numbered cell * 8 + (l - 1) with cells in row-major order; 32 items are four
+// cells, so a lane keeps one direction and steps its cell by four, carrying
+// the cell's coordinates forward instead of dividing them out.
+template <typename T>
+__device__ __forceinline__ void detect_element2_warp(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt,
+                                                     const SurfaceArgs &s, const StepScalars &sc, long long e,
+                                                     uint32_t key_base = 0, uint32_t *owner = nullptr,
+                                                     uint32_t owner_id = 0)
 {
-    constexpr int Q = Lattice<DIM>::Q;
-    uint32_t vid[3] = {0, 0, 0};
-#pragma unroll
-    for (int j = 0; j < DIM; ++j) {
-        vid[j] = s.E[DIM * e + j];
-        if (vid[j] >= (uint32_t)s.nv) { atomicOr(g.status, kStatusBadElement); return; }
+    constexpr int Q = 9;
+    const int lane = threadIdx.x & 31;
+    const uint32_t va = s.E[2 * e], vb = s.E[2 * e + 1];
+    if (va >= (uint32_t)s.nv || vb >= (uint32_t)s.nv) {
+        if (lane == 0) atomicOr(g.status, kStatusBadElement);
+        return;
     }
-    // getBoundingBox: min from FLT_MAX, max from FLT_MIN (sic), then / dx
-    float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
-    float bmax[3] = {1.175494351e-38f, 1.175494351e-38f, 1.175494351e-38f};
+    float bmin[2] = {3.402823466e+38f, 3.402823466e+38f};
+    float bmax[2] = {1.175494351e-38f, 1.175494351e-38f};
+    const uint32_t vid[2] = {va, vb};
 #pragma unroll
-    for (int j = 0; j < DIM; ++j)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            float c = s.V[(size_t)vid[j] * DIM + k];
+        for (int k = 0; k < 2; ++k) {
+            const float c = s.V[(size_t)vid[j] * 2 + k];
             if (c < bmin[k]) bmin[k] = c;
             if (bmax[k] < c) bmax[k] = c;
         }
-    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    const int n[3] = {g.nx, g.ny, g.nz};
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-        lo[k] = max(__float2int_rz(geom::dvd(bmin[k], sc.cl)) - 1, 0);
-        hi[k] = min(__float2int_rz(geom::dvd(bmax[k], sc.cl)) + 1, n[k] - 1);
-    }
-    int cx, cy, cz;
-    dir_vec<DIM>(l, cx, cy, cz);
     const float cl = sc.cl;
-    for (int k3 = lo[2]; k3 <= hi[2]; ++k3)
-        for (int j = lo[1]; j <= hi[1]; ++j)
-            for (int i = lo[0]; i <= hi[0]; ++i) {
-                geom::Hit h;
-                if (DIM == 2) {
-                    h = geom::isect2(s.V, vid[0], vid[1], geom::mul((float)i, cl), geom::mul((float)j, cl),
-                                     geom::mul(geom::sub((float)i, (float)cx), cl),
-                                     geom::mul(geom::sub((float)j, (float)cy), cl));
-                } else {
-                    float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
-                    float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl),
-                                   geom::mul(geom::sub((float)j, (float)cy), cl),
-                                   geom::mul(geom::sub((float)k3, (float)cz), cl)};
-                    h = geom::isect3(s.V, vid[0], vid[1], vid[2], p1, p2);
-                }
-                if (!h.hit) continue;
-                const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
-                insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status, key_base,
-                               owner, owner_id);
-            }
+    const int lo0 = max(__float2int_rz(geom::dvd(bmin[0], cl)) - 1, 0);
+    const int hi0 = min(__float2int_rz(geom::dvd(bmax[0], cl)) + 1, g.nx - 1);
+    const int lo1 = max(__float2int_rz(geom::dvd(bmin[1], cl)) - 1, 0);
+    const int hi1 = min(__float2int_rz(geom::dvd(bmax[1], cl)) + 1, g.ny - 1);
+    const int ext0 = hi0 - lo0 + 1, ext1 = hi1 - lo1 + 1;
+    if (ext0 <= 0 || ext1 <= 0) return;
+    const long long items = (long long)ext0 * ext1 * (Q - 1);
+    const int l = (lane & 7) + 1;
+    int cx, cy, cz;
+    dir_vec<2>(l, cx, cy, cz);
+    int ci = lane >> 3, cj = 0;
+    while (ci >= ext0) { ci -= ext0; ++cj; }
+    for (long long it = lane; it < items; it += 32) {
+        if (it != lane) {
+            ci += 4;
+            while (ci >= ext0) { ci -= ext0; ++cj; }
+        }
+        const int i = lo0 + ci, j = lo1 + cj;
+        const geom::Hit h = geom::isect2(s.V, va, vb, geom::mul((float)i, cl), geom::mul((float)j, cl),
+                                         geom::mul(geom::sub((float)i, (float)cx), cl),
+                                         geom::mul(geom::sub((float)j, (float)cy), cl));
+        if (!h.hit) continue;
+        const uint32_t cell = (uint32_t)((long long)j * g.nx + i);
+        insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status, key_base, owner,
+                       owner_id);
+    }
 }
 
 // Per-vertex force shares of the links of one cell.  Lanes whose links hit

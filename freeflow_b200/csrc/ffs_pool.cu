@@ -195,7 +195,7 @@ struct ffs_pool {
     cudaEvent_t done = nullptr, ev0 = nullptr, ev1 = nullptr;
     bool inflight = false;
     int64_t advances = 0, graph_builds = 0;
-    int sms = 148;
+    int sms = 0;              // SMs of the device, queried at creation
     int grid_dense[kPoolNumShapes] = {};
     int grid_link = 0;        // resident CTAs of the link-cell kernel (one wave)
 };
@@ -249,7 +249,7 @@ ffs_status wait_idle(ffs_pool *p)
 template <typename T> ffs_status capture(ffs_pool *p, int shape, int parity, cudaGraphExec_t *out)
 {
     const int S = p->d.substeps;
-    const int g_kin = p->sms * 4, g_det = p->sms * 8, g_link = p->grid_link, g_fin = p->sms * 2;
+    const int g_kin = p->sms * 4, g_det = p->sms * 4, g_link = p->grid_link, g_fin = p->sms * 2;
     cudaGraph_t graph = nullptr;
     POOL_CK(cudaStreamBeginCapture(p->st, cudaStreamCaptureModeThreadLocal));
     cudaError_t err = cudaSuccess;
