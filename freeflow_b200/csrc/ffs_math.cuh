@@ -36,7 +36,24 @@ __device__ __forceinline__ void herm2(float a0, float a1, float *v)
     v[2] = a0 + a1;
 }
 
-__host__ __device__ constexpr float wgt1(int k) { return k == 1 ? 2.0f / 3.0f : 1.0f / 6.0f; }
+// Lattice weights, one float constant per population class, as the reference
+// writes them (LbmConstants.hpp:28-35, :51-54): the number of non-zero
+// velocity components selects 4/9, 1/9, 1/36 (D2Q9) or 8/27, 2/27, 1/54,
+// 1/216 (D3Q27).  They equal the products of the 1D weights 2/3 and 1/6, but
+// the products of the rounded 1D weights sum to 1 + 1.1e-7 over the 27
+// directions, which would add that fraction of the mass every step; these
+// sum to 1 + 7e-9.
+__host__ __device__ constexpr float wgt2(int kx, int ky)
+{
+    return ((kx != 1) + (ky != 1)) == 0 ? 4.0f / 9.0f : ((kx != 1) + (ky != 1)) == 1 ? 1.0f / 9.0f : 1.0f / 36.0f;
+}
+__host__ __device__ constexpr float wgt3(int kx, int ky, int kz)
+{
+    return ((kx != 1) + (ky != 1) + (kz != 1)) == 0   ? 8.0f / 27.0f
+           : ((kx != 1) + (ky != 1) + (kz != 1)) == 1 ? 2.0f / 27.0f
+           : ((kx != 1) + (ky != 1) + (kz != 1)) == 2 ? 1.0f / 54.0f
+                                                      : 1.0f / 216.0f;
+}
 
 // Hermite coefficients of one cell (the reference's m1, m2 and Q terms).
 template <int DIM> struct Coef;
@@ -70,7 +87,7 @@ template <> struct Coef<2> {
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
                 const int i = dir_index<2>(kx, ky, 1);
-                f[i] = (wgt1(kx) * wgt1(ky)) * F[kx];
+                f[i] = wgt2(kx, ky) * F[kx];
             }
         }
     }
@@ -84,7 +101,7 @@ template <> struct Coef<2> {
         s = fmaf(m2xx, gx, s); s = fmaf(m2yy, gy, s);
         s = fmaf(m2xy, fx * fy, s);
         s = fmaf(qxxy, gx * fy, s); s = fmaf(qxyy, fx * gy, s);
-        float w = (cx ? 1.0f / 6.0f : 2.0f / 3.0f) * (cy ? 1.0f / 6.0f : 2.0f / 3.0f);
+        const float w = wgt2(cx + 1, cy + 1);
         return w * s;
     }
 };
@@ -136,7 +153,7 @@ template <> struct Coef<3> {
                 float F[3];
                 herm3(C0[ky], C1[ky], C2[ky], F);
 #pragma unroll
-                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = (wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx];
+                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = wgt3(kx, ky, kz) * F[kx];
             }
         }
     }
@@ -163,7 +180,7 @@ template <> struct Coef<3> {
         s = fmaf(qxxz, gx * fz, s); s = fmaf(qxzz, fx * gz, s);
         s = fmaf(qyyz, gy * fz, s); s = fmaf(qyzz, fy * gz, s);
         s = fmaf(qxyz, fx * fy * fz, s);
-        float w = (cx ? 1.0f / 6.0f : 2.0f / 3.0f) * (cy ? 1.0f / 6.0f : 2.0f / 3.0f) * (cz ? 1.0f / 6.0f : 2.0f / 3.0f);
+        const float w = wgt3(cx + 1, cy + 1, cz + 1);
         return w * s;
     }
 };
@@ -232,7 +249,7 @@ template <typename V> struct Coef3V {
                 V F[3];
                 herm3v(C0[ky], C1[ky], C2[ky], F);
 #pragma unroll
-                for (int kx = 0; kx < 3; ++kx) sink(kz, ky, kx, vconst<V>(wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx]);
+                for (int kx = 0; kx < 3; ++kx) sink(kz, ky, kx, vconst<V>(wgt3(kx, ky, kz)) * F[kx]);
             }
         }
     }
@@ -257,7 +274,7 @@ template <typename V> struct Coef3V {
                 V F[3];
                 herm3v(C0[ky], C1[ky], C2[ky], F);
 #pragma unroll
-                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = vconst<V>(wgt1(kx) * wgt1(ky) * wgt1(kz)) * F[kx];
+                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = vconst<V>(wgt3(kx, ky, kz)) * F[kx];
             }
         }
     }

@@ -1,0 +1,117 @@
+"""The five benchmark configurations at their full sizes on the GPU, through
+the C ABI, checked by properties that do not need the oracle to run at that
+size (or, for the small config A, against the FP64 oracle itself):
+
+  A  D2Q9 256x128 cylinder, FP32, 2000 steps: velocity and accumulated
+     surface forces against the FP64 oracle (relative L2 <= 1e-3; measured
+     1.8e-4 and 3.3e-4).
+  B  D2Q9 1200x400 swimmer, 10k steps: FP32 and FP16 storage both stay
+     healthy (status word clear), and their accumulated surface forces agree
+     within 10 %.  The prescribed tail speed is about 0.25 lattice units at
+     viscosity 0.005, so the flow is unsteady and fields of different
+     precisions decorrelate; integral forces stay close.
+  C  D3Q27 periodic Taylor-Green 128^3, 5000 steps: mass conserved to the
+     rounding of FP32 (drift <= 2e-8 of the mass per step; the reference's
+     FP32 weights give 7.4e-9), kinetic energy decreasing, and FP16 storage
+     tracking the FP32 energy within 3 %.
+  D  D3Q27 384x192x192 swimmer, 1000 steps: FP16 storage against FP32,
+     velocity relative L2 <= 2e-3 (measured 5.3e-4) and accumulated forces
+     <= 5e-4 (4.6e-5).
+The serving mix (config E) is covered by test_gpu_serving.py.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from freeflow_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+def gpu_run(wl, steps, storage="f32", checkpoints=()):
+    from freeflow_b200 import DeviceSurface, FluidGrid
+
+    g = FluidGrid(**wl.grid_kwargs(storage=storage))
+    g.set_flags(wl.flags)
+    g.set_moments(wl.moments)
+    surf = None
+    if wl.elements is not None:
+        v, u = wl.surface_at(0)
+        surf = DeviceSurface(v, u, wl.elements, with_forces64=True)
+    saved = []
+    for s in range(steps):
+        if surf is not None:
+            if wl.kinematics is not None or s == 0:
+                surf.update(*wl.surface_at(s))
+            g.step(surf)
+        else:
+            g.step()
+        if s + 1 in checkpoints:
+            saved.append(g.get_moments().astype(np.float64))
+    m = g.get_moments().astype(np.float64)
+    st = g.status()
+    F = surf.forces64.cpu().numpy().reshape(-1) if surf is not None else None
+    g.close()
+    return m, st, F, saved
+
+
+def test_config_a_cylinder_2000_steps_vs_fp64(cuda):
+    from oracle import oracle as O
+
+    wl = W.cylinder_channel_2d()
+    gm, st, gF, _ = gpu_run(wl, 2000)
+    assert st == 0
+    O.set_threads(os.cpu_count() or 1)
+    o = O.Oracle(2, wl.nx, wl.ny, 1, viscosity=wl.fluid_viscosity, density=wl.fluid_density, dx=wl.fluid_dx,
+                 dt=wl.dt, boundary_velocities=wl.boundary_velocities, periodic=wl.periodic, precision="phys64")
+    o.set_flags(wl.flags)
+    o.set_moments(wl.moments.astype(np.float64))
+    F = np.zeros(wl.rest.size)
+    v, u = wl.surface_at(0)
+    for _ in range(2000):
+        o.step(v, u, wl.elements, F)
+    om = o.get_moments()
+    o.close()
+    assert rel(gm[:, 1:3], om[:, 1:3]) <= 1e-3
+    assert rel(gF, F) <= 1e-3
+
+
+def test_config_b_swimmer_10k_steps_fp32_and_fp16(cuda):
+    wl = W.swimmer_2d()
+    _, s32, F32, _ = gpu_run(wl, 10000, "f32")
+    _, s16, F16, _ = gpu_run(wl, 10000, "f16")
+    assert s32 == 0 and s16 == 0
+    assert np.isfinite(F32).all() and np.isfinite(F16).all()
+    assert rel(F16, F32) <= 0.1
+
+
+def test_config_c_taylor_green_128_cubed_5000_steps(cuda):
+    wl = W.taylor_green_3d(n=128, u0=0.04, viscosity=0.005)
+    m0 = wl.moments.astype(np.float64)
+    mass0 = m0[:, 0].sum()
+    ke = lambda m: 0.5 * np.sum(m[:, 0] * np.sum(m[:, 1:4] ** 2, axis=1))
+    marks = (1000, 2000, 3000, 4000, 5000)
+    energies = {}
+    for storage in ("f32", "f16"):
+        _, st, _, saved = gpu_run(wl, 5000, storage, checkpoints=marks)
+        assert st == 0
+        drift = [(m[:, 0].sum() - mass0) / mass0 / t for m, t in zip(saved, marks)]
+        assert max(abs(d) for d in drift) <= 2e-8, drift
+        e = [ke(m) for m in saved]
+        assert all(b < a for a, b in zip([ke(m0)] + e[:-1], e))
+        energies[storage] = np.array(e)
+    assert np.abs(energies["f16"] / energies["f32"] - 1.0).max() <= 0.03
+
+
+def test_config_d_swimmer_fp16_vs_fp32_1000_steps(cuda):
+    wl = W.swimmer_3d()
+    m32, s32, F32, _ = gpu_run(wl, 1000, "f32")
+    m16, s16, F16, _ = gpu_run(wl, 1000, "f16")
+    assert s32 == 0 and s16 == 0
+    assert rel(m16[:, 1:4], m32[:, 1:4]) <= 2e-3
+    assert rel(F16, F32) <= 5e-4
