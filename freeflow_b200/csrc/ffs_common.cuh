@@ -266,6 +266,32 @@ __device__ __forceinline__ void encode_store_strided(const float *m, T *base, si
     }
 }
 
+// Same as encode_store with planes[k] = base + k * stride and a 32-bit index
+// idx + k * stride (the caller guarantees it fits).
+template <int DIM, typename T>
+__device__ __forceinline__ void encode_store_idx32(const float *m, T *base, uint32_t idx, uint32_t stride,
+                                                   const Codec &c)
+{
+    constexpr int NM = Lattice<DIM>::NM;
+    if constexpr (!StorageTraits<T>::kEncoded) {
+#pragma unroll
+        for (int k = 0; k < NM; ++k) base[idx + (uint32_t)k * stride] = StorageTraits<T>::to(m[k]);
+    } else {
+        float ud[DIM];
+        base[idx] = StorageTraits<T>::to(m[0] - 1.0f);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            T s = StorageTraits<T>::to(m[1 + a] * c.su);
+            base[idx + (uint32_t)(1 + a) * stride] = s;
+            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
+        }
+#pragma unroll
+        for (int k = DIM + 1; k < NM; ++k)
+            base[idx + (uint32_t)k * stride] =
+                StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+    }
+}
+
 // The values encode_store writes, as they read back: m itself for FP32, the
 // decoded rounded deviations otherwise.
 template <int DIM, typename T>

@@ -15,13 +15,19 @@ from helpers import max_abs, run_pair
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [0, 1, 2]
+# (variant, index width): the single-plane variants run with 32-bit indices on
+# grids of up to 429 M cells and 64-bit ones beyond; FFS_DENSE3D_INDEX64 forces
+# the 64-bit path here
+VARIANTS = [(0, 32), (1, 32), (2, 64), (0, 64), (1, 64)]
 
 
-@pytest.fixture(params=VARIANTS)
+@pytest.fixture(params=VARIANTS, ids=lambda v: f"v{v[0]}-i{v[1]}")
 def variant(request, monkeypatch):
-    monkeypatch.setenv("FFS_DENSE3D_VARIANT", str(request.param))
-    return request.param
+    v, width = request.param
+    monkeypatch.setenv("FFS_DENSE3D_VARIANT", str(v))
+    if width == 64:
+        monkeypatch.setenv("FFS_DENSE3D_INDEX64", "1")
+    return v
 
 
 def test_swimmer(cuda, variant):
