@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *
 //     iteration after row o+1 was reconstructed, which leaves one barrier per
 //     row.
 // The per-cell arithmetic is dense2d_recon / dense2d_update_cell, the same
-// code as the tile kernel, so both give the same bits.
+// code as the tile kernel, so both give the same bits.  Episodes hold fewer
+// than 2^22 cells, so every moment index fits in 32 bits.
 template <typename T, int TX, int CH, int DEPTH>
 __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
 {
@@ -190,17 +191,18 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
         auto issue = [&](int r) {
             if (r <= ye) {
                 T (*st)[kSW] = stage[(r + kStage) % kStage];
-                const size_t row = (size_t)halo_index(r, g.ny, wy) * g.nx;
+                const uint32_t row = (uint32_t)halo_index(r, g.ny, wy) * (uint32_t)g.nx;
                 if (vec) {
                     for (int e = tid; e < 6 * kCopies; e += TX) {
                         const int k = e / kCopies, w = e - k * kCopies;
                         const int x = xs + w * kPer;
-                        if (x + kPer <= g.nx) cp_async16(&st[k][w * kPer], g.src + (size_t)k * g.ncell + row + x);
+                        if (x + kPer <= g.nx)
+                            cp_async16(&st[k][w * kPer], g.src + ((uint32_t)k * g.ncell + row + (uint32_t)x));
                     }
                 } else {
                     for (int e = tid; e < 6 * kSW; e += TX) {
                         const int k = e / kSW, j = e - k * kSW;
-                        if (xs + j < g.nx) st[k][j] = g.src[(size_t)k * g.ncell + row + xs + j];
+                        if (xs + j < g.nx) st[k][j] = g.src[(uint32_t)k * g.ncell + row + (uint32_t)(xs + j)];
                     }
                 }
             }
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
         // that of row r-2 (updated this iteration) and f8n that of row r-1;
         // row r's is loaded at the end of iteration r, two iterations ahead
         auto flag_at = [&](int y) -> uint32_t {
-            return (owner && y >= yb && y < ye) ? (uint32_t)g.flags[(size_t)y * g.nx + x] : 0u;
+            return (owner && y >= yb && y < ye) ? (uint32_t)g.flags[(uint32_t)y * (uint32_t)g.nx + (uint32_t)x] : 0u;
         };
         uint32_t f8 = 0, f8n = 0;
         for (int r = yb - 1; r <= ye + 1; ++r) {
@@ -249,7 +251,7 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
             const int o = r - 2;
             if (o >= yb && owner && is_updated(f8 & kTypeMask) && !(f8 & kBitLink)) {
                 const uint32_t idx = (uint32_t)(o * g.nx + x);
-                dense2d_update_cell(
+                dense2d_update_cell<T, true>(
                     g, idx, f8, [&](int i) { return ring[(o - L::cy(i) + kRing) % kRing][i][tid - L::cx(i)]; },
                     [&](int i) { return ring[(o + kRing) % kRing][i][tid]; });
             }

@@ -74,8 +74,10 @@ __device__ __forceinline__ void dense2d_recon(const GridArgs<T> &g, const T (&ra
 // SolidDynamic, no moving-boundary link): pull(i) is the reconstructed
 // population i of the upstream cell x - c_i and own(i) that of the cell
 // itself.  Bounce-back, clamp, raw moments, collision, store and the outlet
-// feed follow FsiCoupling2D.cu:154-252.
-template <typename T, typename Pull, typename Own>
+// feed follow FsiCoupling2D.cu:154-252.  IDX32: every moment index
+// k * ncell + idx fits in 32 bits (the caller guarantees it), so the stores
+// take 32-bit indices instead of six 64-bit plane pointers.
+template <typename T, bool IDX32 = false, typename Pull, typename Own>
 __device__ __forceinline__ void dense2d_update_cell(const GridArgs<T> &g, uint32_t idx, uint32_t f8, Pull &&pull,
                                                     Own &&own)
 {
@@ -95,10 +97,14 @@ __device__ __forceinline__ void dense2d_update_cell(const GridArgs<T> &g, uint32
     float R[6], m[6];
     raw_moments2(pop, R);
     collide2(R, g.omega, m);
-    T *planes[6];
+    if constexpr (IDX32) {
+        encode_store_idx32<2, T>(m, g.dst, idx, g.ncell, g.codec);
+    } else {
+        T *planes[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
-    encode_store<2, T>(m, planes, idx, g.codec);
+        for (int k = 0; k < 6; ++k) planes[k] = g.dst + (size_t)k * g.ncell;
+        encode_store<2, T>(m, planes, idx, g.codec);
+    }
     if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
     if (f8 & kBitOutletSrc) {
         float ms[6];
