@@ -36,6 +36,7 @@ import os
 import sys
 import warnings
 from dataclasses import dataclass, field
+from typing import Optional
 
 import numpy as np
 
@@ -113,8 +114,13 @@ class fem:  # noqa: N801 -- the reference's submodule name
 
 @dataclass
 class BoundaryCondition:
+    """One "boundaries" entry: the cell at `position` (Config.hpp:23-62).  `to`
+    is an extension of the JSON format: when an entry also has "to", it
+    covers the inclusive box from "pos" to "to" (a wall row of a 1200-cell
+    channel is then one entry instead of 1200)."""
     position: list
     flag: int
+    to: Optional[list] = None
 
 
 @dataclass
@@ -217,7 +223,8 @@ def params_from_json(j: dict, dim: int):
         if not isinstance(bc, dict):
             warnings.warn("item in 'boundaries' is not an object; skipped")
             continue
-        p.boundaries.append(BoundaryCondition([int(x) for x in bc["pos"]], NODE_FLAGS.get(bc["type"], 0)))
+        to = [int(x) for x in bc["to"]] if "to" in bc else None
+        p.boundaries.append(BoundaryCondition([int(x) for x in bc["pos"]], NODE_FLAGS.get(bc["type"], 0), to))
     for s in j.get("solids", []) or []:
         if isinstance(s, dict):
             p.solids.append(_solid(s, dim))
@@ -277,18 +284,28 @@ class Config3D(_ConfigBase):
 
 def flags_from_params(p) -> np.ndarray:
     """Per-cell node flags: Fluid everywhere, then each boundary entry in file order (a later entry
-    wins); entries outside the grid are ignored (LbmInitializer2D.cu:103-124 and its 3D twin)."""
+    wins); entries outside the grid are ignored (LbmInitializer2D.cu:103-124 and its 3D twin).
+    An entry with `to` sets every cell of its box, clipped to the grid."""
     dim = 2 if isinstance(p, SimulationParameters2D) else 3
     nx, ny, nz = p.fluid_nx, p.fluid_ny, (p.fluid_nz if dim == 3 else 1)
-    f = np.full(nx * ny * nz, FLUID, dtype=np.uint8)
+    f = np.full((nz, ny, nx), FLUID, dtype=np.uint8)
     for bc in p.boundaries:
-        x, y = bc.position[0], bc.position[1]
-        z = bc.position[2] if dim == 3 else 0
-        if 0 <= x < nx and 0 <= y < ny and 0 <= z < nz:
-            f[(z * ny + y) * nx + x] = bc.flag
-        else:
-            warnings.warn(f"boundary condition at {bc.position} is outside the grid and is ignored")
-    return f
+        lo = list(bc.position[:dim]) + [0] * (3 - dim)
+        if bc.to is None:
+            x, y, z = lo
+            if 0 <= x < nx and 0 <= y < ny and 0 <= z < nz:
+                f[z, y, x] = bc.flag
+            else:
+                warnings.warn(f"boundary condition at {bc.position} is outside the grid and is ignored")
+            continue
+        hi = list(bc.to[:dim]) + [0] * (3 - dim)
+        a = [max(min(lo[k], hi[k]), 0) for k in range(3)]
+        b = [min(max(lo[k], hi[k]), n - 1) for k, n in enumerate((nx, ny, nz))]
+        if any(a[k] > b[k] for k in range(3)):
+            warnings.warn(f"boundary box {bc.position}..{bc.to} is outside the grid and is ignored")
+            continue
+        f[a[2]:b[2] + 1, a[1]:b[1] + 1, a[0]:b[0] + 1] = bc.flag
+    return f.reshape(-1)
 
 
 # ------------------------------------------------------------- simulators

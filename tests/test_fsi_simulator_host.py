@@ -74,6 +74,31 @@ def test_flags_from_boundaries_later_entry_wins_and_outside_is_ignored():
     assert f3[(1 * 2 + 1) * 3 + 2] == 24 and (f3 == F.FLUID).sum() == 11
 
 
+def test_boundary_boxes_equal_their_cells(tmp_path):
+    """A "boundaries" entry with "to" covers its inclusive box: the channel walls,
+    inlet and outlet of a 40x12 grid as four entries give the same flags as the
+    reference's one entry per cell (and later entries still win)."""
+    nx, ny = 40, 12
+    cells = ([{"type": "Wall", "pos": [x, y]} for y in (0, ny - 1) for x in range(nx)]
+             + [{"type": "InletLeft", "pos": [0, y]} for y in range(1, ny - 1)]
+             + [{"type": "OutletRight", "pos": [nx - 1, y]} for y in range(1, ny - 1)])
+    boxes = [{"type": "Wall", "pos": [0, 0], "to": [nx - 1, 0]}, {"type": "Wall", "pos": [nx - 1, ny - 1], "to": [0, ny - 1]},
+             {"type": "InletLeft", "pos": [0, 1], "to": [0, ny - 2]}, {"type": "OutletRight", "pos": [nx - 1, 1], "to": [nx - 1, ny - 2]}]
+    flags = []
+    for entries in (cells, boxes):
+        c = F.Config2D()
+        assert c.load(_write(tmp_path, "b.json", {"fluid_nx": nx, "fluid_ny": ny, "boundaries": entries}))
+        flags.append(F.flags_from_params(c.get_params()))
+    assert np.array_equal(flags[0], flags[1])
+    assert (flags[1] != F.FLUID).sum() == 2 * nx + 2 * (ny - 2)
+    p3 = F.SimulationParameters3D(fluid_nx=6, fluid_ny=5, fluid_nz=4)
+    p3.boundaries = [F.BoundaryCondition([0, 0, 0], 5, [5, 4, 0]), F.BoundaryCondition([2, 2, 0], 13),
+                     F.BoundaryCondition([-3, 1, 1], 24, [1, 1, 9])]
+    f3 = F.flags_from_params(p3).reshape(4, 5, 6)
+    assert (f3[0] == 5).sum() == 29 and f3[0, 2, 2] == 13
+    assert (f3[1:, 1, :2] == 24).all() and (f3 == 24).sum() == 6
+
+
 def _square_mesh(n):
     xs = np.linspace(0.0, 1.0, n + 1)
     v = np.array([[x, y] for y in xs for x in xs])
