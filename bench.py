@@ -10,9 +10,9 @@ fraction of the measured HBM peak.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload D|C|B|A] [--storage f32|f16|bf16] [--small]
 
-N > 1 runs one independent replica per GPU (the single-grid path has no
-exchange step; see DESIGN.md "multi-GPU"), launched by torchrun; the time is
-the max over ranks and value = all cells updated / that time ("weak").
+N > 1 runs one independent replica per GPU (one grid per GPU: the grid is not
+sharded, so there is no exchange step), launched by torchrun; the time is the
+max over ranks and value = all cells updated / that time ("weak").
 
 ``--impl reference`` times the reference's algorithm on the host cores: the
 FP32 restatement in oracle/ (the reference's CUDA sources do not build here)
