@@ -163,7 +163,7 @@ template <int DIM> constexpr int kLinkGroup = DIM == 2 ? 16 : 32;
 // collides, stores and feeds outlets.  `links` holds the Q keys of the
 // cell's table slot; the force shares go to `acc`.  Every lane of the warp
 // calls this together (the force sums and the reduction are warp-wide); a
-// group with valid = false has no cell this round and only takes part in
+// group with valid = false has no cell in this iteration and only takes part in
 // those, with arguments that still name a real cell.
 template <int DIM, typename T, bool HALF>
 __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const unsigned long long *links,
