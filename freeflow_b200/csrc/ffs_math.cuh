@@ -132,42 +132,6 @@ template <> struct Coef<3> {
         float t = fmaf(pxy, uz, fmaf(pyz, ux, pxz * uy));
         qxyz = 27.0f * r * fmaf(-2.0f * ux * uy, uz, t);
     }
-    // The 27 populations, sorted by slice: out[kz][ky][kx] with k = c + 1.
-    __device__ __forceinline__ void populations_xyz(float (*out)[3][3]) const
-    {
-        float B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
-        herm3(rho, m1z, m2zz, B00);
-        herm3(m1x, m2xz, qxzz, B10);
-        herm3(m1y, m2yz, qyzz, B01);
-        herm2(m2xx, qxxz, B20);
-        herm2(m2yy, qyyz, B02);
-        herm2(m2xy, qxyz, B11);
-#pragma unroll
-        for (int kz = 0; kz < 3; ++kz) {
-            float C0[3], C1[3], C2[3];
-            herm3(B00[kz], B01[kz], B02[kz], C0);
-            herm3(B10[kz], B11[kz], qxyy, C1);
-            herm2(B20[kz], qxxy, C2);
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                float F[3];
-                herm3(C0[ky], C1[ky], C2[ky], F);
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = wgt3(kx, ky, kz) * F[kx];
-            }
-        }
-    }
-    __device__ __forceinline__ void populations(float *f) const
-    {
-        float o[3][3][3];
-        populations_xyz(o);
-#pragma unroll
-        for (int kz = 0; kz < 3; ++kz)
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky)
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) f[dir_index<3>(kx, ky, kz)] = o[kz][ky][kx];
-    }
     __device__ __forceinline__ float population(int cx, int cy, int cz) const
     {
         float gx = cx ? 1.0f : -0.5f, gy = cy ? 1.0f : -0.5f, gz = cz ? 1.0f : -0.5f;
@@ -253,31 +217,6 @@ template <typename V> struct Coef3V {
             }
         }
     }
-    // out[kz][ky][kx], k = c + 1
-    __device__ __forceinline__ void populations_xyz(V (*out)[3][3]) const
-    {
-        V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
-        herm3v(rho, m1z, m2zz, B00);
-        herm3v(m1x, m2xz, qxzz, B10);
-        herm3v(m1y, m2yz, qyzz, B01);
-        herm2v(m2xx, qxxz, B20);
-        herm2v(m2yy, qyyz, B02);
-        herm2v(m2xy, qxyz, B11);
-#pragma unroll
-        for (int kz = 0; kz < 3; ++kz) {
-            V C0[3], C1[3], C2[3];
-            herm3v(B00[kz], B01[kz], B02[kz], C0);
-            herm3v(B10[kz], B11[kz], qxyy, C1);
-            herm2v(B20[kz], qxxy, C2);
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                V F[3];
-                herm3v(C0[ky], C1[ky], C2[ky], F);
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) out[kz][ky][kx] = vconst<V>(wgt3(kx, ky, kz)) * F[kx];
-            }
-        }
-    }
 };
 
 // ------------------------------------------------------------ raw moments
@@ -295,42 +234,6 @@ __device__ __forceinline__ void raw_moments2(const float *f, float *R)
     R[3] = s0 + (s1 + sm);      // Pxx
     R[4] = sy;                  // Pyy
     R[5] = d1 - dm;             // Pxy
-}
-
-__device__ __forceinline__ void raw_moments3(const float (*F)[3][3], float *R)
-{
-    // F[kz][ky][kx]; stage x
-    float X0[3][3], X1[3][3], X2[3][3];
-#pragma unroll
-    for (int kz = 0; kz < 3; ++kz)
-#pragma unroll
-        for (int ky = 0; ky < 3; ++ky) {
-            float s = F[kz][ky][2] + F[kz][ky][0];
-            X1[kz][ky] = F[kz][ky][2] - F[kz][ky][0];
-            X2[kz][ky] = s;
-            X0[kz][ky] = F[kz][ky][1] + s;
-        }
-    // stage y: Y[p][q][kz]
-    float Y00[3], Y01[3], Y02[3], Y10[3], Y11[3], Y20[3];
-#pragma unroll
-    for (int kz = 0; kz < 3; ++kz) {
-        float s0 = X0[kz][2] + X0[kz][0];
-        Y00[kz] = X0[kz][1] + s0; Y01[kz] = X0[kz][2] - X0[kz][0]; Y02[kz] = s0;
-        float s1 = X1[kz][2] + X1[kz][0];
-        Y10[kz] = X1[kz][1] + s1; Y11[kz] = X1[kz][2] - X1[kz][0];
-        Y20[kz] = X2[kz][1] + (X2[kz][2] + X2[kz][0]);
-    }
-    float s = Y00[2] + Y00[0];
-    R[0] = Y00[1] + s;                    // rho   M000
-    R[3] = Y00[2] - Y00[0];               // jz    M001
-    R[6] = s;                             // Pzz   M002
-    R[2] = Y01[1] + (Y01[2] + Y01[0]);    // jy    M010
-    R[8] = Y01[2] - Y01[0];               // Pyz   M011
-    R[5] = Y02[1] + (Y02[2] + Y02[0]);    // Pyy   M020
-    R[1] = Y10[1] + (Y10[2] + Y10[0]);    // jx    M100
-    R[9] = Y10[2] - Y10[0];               // Pxz   M101
-    R[7] = Y11[1] + (Y11[2] + Y11[0]);    // Pxy   M110
-    R[4] = Y20[1] + (Y20[2] + Y20[0]);    // Pxx   M200
 }
 
 // ------------------------------------------------------------- collision
