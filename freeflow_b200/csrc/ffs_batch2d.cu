@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, 
 
 // ------------------------------------------------------------ link cells
 template <typename T>
-__global__ void __launch_bounds__(256, 3) pool_link_cells_kernel(const PoolEpisode *eps, LinkTable lt,
+__global__ void __launch_bounds__(256, 4) pool_link_cells_kernel(const PoolEpisode *eps, LinkTable lt,
                                                                  const uint32_t *owner, int parity)
 {
     constexpr int Q = 9, G = kLinkGroup<2>, kPerWarp = 32 / G;
