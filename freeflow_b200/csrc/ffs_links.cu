@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) detect_links2_kernel(GridArgs<T> g, uint3
 
 // -------------------------------------------------------------- link cells
 template <int DIM, typename T, bool HALF>
-__global__ void __launch_bounds__(256, 4) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
+__global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
                                                          StepScalars sc)
 {
     constexpr int Q = Lattice<DIM>::Q, G = kLinkGroup<DIM>, kPerWarp = 32 / G;
