@@ -47,15 +47,17 @@ def _run_pool(pool, slots_specs, control_steps):
     return outs
 
 
-@pytest.mark.parametrize("shape", TILES + STRIPS)
-def test_pool_f32_matches_single_grid_step(cuda, pin_shape, shape):
+@pytest.mark.parametrize("shape,storage", [(s, "f32") for s in TILES + STRIPS] + [(1, "f16"), (6, "f16"), (6, "bf16")])
+def test_pool_f32_matches_single_grid_step(cuda, pin_shape, shape, storage):
+    """Pool episodes against single grids of the same storage (FP32, and the
+    16-bit paths with their codec), unit by unit: identical bits."""
     pin_shape(shape)
     specs = [S.make_episode(256, 128, seed=11, length=10), S.make_episode(512, 192, seed=12, length=10)]
-    pool = S.Pool(storage="f32", budget_bytes=1 << 30, max_episodes=8)
+    pool = S.Pool(storage=storage, budget_bytes=1 << 30, max_episodes=8)
     slots = [(pool.admit(sp), sp) for sp in specs]
     outs = _run_pool(pool, slots, 3)
     for (s, sp) in slots:
-        env = S.PlainEnv(sp)
+        env = S.PlainEnv(sp, storage)
         for c in range(3):
             env.set_action(_actions(sp, c))
             F = env.control_step(pool.substeps)
