@@ -79,3 +79,24 @@ def test_odd_and_chunked_depths(cuda, variant, nz):
     gm, om, _, _, st = run_pair(wl, 4)
     assert st == 0
     assert max_abs(gm, om) <= 4e-6
+
+
+def test_periodic_width_not_a_tile_multiple(cuda, variant):
+    """nx = 48 with x periodic: the last tile's halo wraps onto the first
+    columns, and its cells beyond nx only serve as halo."""
+    wl = W.taylor_green_3d(n=48, u0=0.04, viscosity=0.01)
+    nm = wl.moments.shape[1]
+    wl.moments = np.ascontiguousarray(wl.moments.reshape(48, 48, 48, nm)[:12, :20, :].reshape(-1, nm))
+    wl.flags = np.ascontiguousarray(wl.flags.reshape(48, 48, 48)[:12, :20, :].reshape(-1))
+    wl.ny, wl.nz = 20, 12
+    gm, om, _, _, st = run_pair(wl, 6)
+    assert st == 0
+    assert max_abs(gm, om) <= 2e-6
+
+
+def test_odd_width(cuda, variant):
+    """nx odd: rows whose cells do not pair up on 8-byte boundaries."""
+    wl = W.swimmer_3d(nx=41, ny=24, nz=20, body_frac=0.3, nlat=8, nlon=12, seed=11)
+    gm, om, _, _, st = run_pair(wl, 4)
+    assert st == 0
+    assert max_abs(gm, om) <= 4e-6
