@@ -20,6 +20,10 @@ with all host threads, each step a z-slab sample of the same workload.
 
 The default line (N = 1) also carries:
   storage                 config D with FP16 and BF16 moment storage (GPU);
+  coupled_step            config D stepped through ffs_lbm_step_coupled
+                          (surface gathered from a volume mesh, forces
+                          scattered back, one stream) against the same stages
+                          with the reference's two host synchronisations (GPU);
   serving                 config E, the batched FP16 pool against the plain
                           per-episode FP32 path (GPU);
   cpu_baseline and        the CPU leg, the only part of the GPU arm that runs
@@ -437,6 +441,70 @@ def run_storage_d(wl: W.Workload, storage: str, steps: int = 40, warmup: int = 5
             "device_status": status}
 
 
+def run_coupled(wl: W.Workload, steps: int = 40, warmup: int = 5):
+    """The coupled step (surface gathered from a volume mesh, fluid step, forces
+    scattered back) on config D, against the same three stages issued the way
+    the reference's Simulator3D::step issues them: gather, stream synchronise,
+    fluid step, zero + scatter + zero, stream synchronise.  The volume mesh is
+    the surface plus as many interior vertices; the body moves as in the main
+    measurement (per-step volume arrays resident on the device).  CUDA events
+    bracket each loop, so the host synchronisations show up as device idle
+    time."""
+    import torch
+    from freeflow_b200 import DeviceSurface, FluidGrid, VolumeSurface
+
+    nv = wl.rest.shape[0]
+    nvol = 2 * nv
+    perm = np.random.default_rng(1).permutation(nvol)[:nv].astype(np.uint32)
+    n = steps + warmup
+    vp = np.zeros((n, nvol, 3), np.float32)
+    vv = np.zeros((n, nvol, 3), np.float32)
+    for s in range(n):
+        vp[s, perm], vv[s, perm] = wl.surface_at(s)
+    VP, VV = torch.from_numpy(vp).cuda(), torch.from_numpy(vv).cuda()
+    idx = torch.from_numpy(perm.astype(np.int64)).cuda()
+    stream = torch.cuda.Stream()
+    out = {}
+    for mode in ("coupled", "synchronised"):
+        g = FluidGrid(**wl.grid_kwargs())
+        g.set_flags(wl.flags)
+        g.set_moments(wl.moments)
+        vol = VolumeSurface(vp[0], vv[0], perm, wl.elements)
+        surf = DeviceSurface(vp[0][perm], vv[0][perm], wl.elements)
+        g.reserve_surface(nv, max(4096, surf.num_elements * 40))
+
+        def step(s):
+            if mode == "coupled":
+                vol.volume_positions, vol.volume_velocities = VP[s], VV[s]
+                g.step_coupled(vol, stream=stream)
+            else:
+                torch.index_select(VP[s], 0, idx, out=surf.vertices)
+                torch.index_select(VV[s], 0, idx, out=surf.velocities)
+                stream.synchronize()
+                g.step(surf, stream=stream)
+                vol.volume_forces.zero_()
+                vol.volume_forces.index_copy_(0, idx, surf.forces)
+                surf.forces.zero_()
+                stream.synchronize()
+
+        with torch.cuda.stream(stream):
+            for s in range(warmup):
+                step(s)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for s in range(steps):
+                step(warmup + s)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        out[mode] = {"ms_per_step": round(e0.elapsed_time(e1) / steps, 4), "device_status": g.status(clear=True)}
+        g.close()
+    out["case"] = (f"{wl.name}, {nvol}-vertex volume mesh ({nv} on the surface), {steps} steps; synchronised = "
+                   "gather, sync, step, zero + scatter + zero, sync per step")
+    return out
+
+
 def run_serving_line(args):
     """`--workload E`: the serving measurement as its own JSON line."""
     import torch
@@ -644,6 +712,7 @@ def run_ours(args):
             out["storage_errors_vs_fp64"] = errors
         if world == 1 and not args.small and args.workload == "D" and storage == "f32":
             out["storage"] = {st: run_storage_d(wl, st) for st in ("f16", "bf16")}
+            out["coupled_step"] = run_coupled(wl)
         if world == 1 and not args.no_serving and not args.small:
             out["serving"] = run_serving(iterations=150, warmup=20)
         print(json.dumps(out), flush=True)

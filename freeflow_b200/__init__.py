@@ -6,6 +6,6 @@ binding, and host-side mirrors of the reference's Python interface.
 """
 from . import _capi
 from ._capi import FfsError, load
-from .grid import DeviceSurface, FluidGrid
+from .grid import DeviceSurface, FluidGrid, VolumeSurface
 
-__all__ = ["FluidGrid", "DeviceSurface", "FfsError", "load", "_capi"]
+__all__ = ["FluidGrid", "DeviceSurface", "VolumeSurface", "FfsError", "load", "_capi"]

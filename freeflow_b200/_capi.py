@@ -33,7 +33,7 @@ NOALLOC_MAX_LINK_CELLS = 16384
 EXPORTS = (
     "ffs_lbm_create", "ffs_lbm_destroy", "ffs_lbm_set_flags", "ffs_lbm_get_flags", "ffs_lbm_initialize",
     "ffs_lbm_set_moments", "ffs_lbm_get_moments", "ffs_lbm_reserve_surface", "ffs_lbm_step",
-    "ffs_lbm_step_noalloc",
+    "ffs_lbm_step_noalloc", "ffs_lbm_step_coupled",
     "ffs_lbm_fill_solid", "ffs_lbm_get_status", "ffs_lbm_get_info", "ffs_lbm_debug_links",
     "ffs_lbm_profile_enable", "ffs_lbm_profile_read",
     "ffs_status_string", "ffs_last_error", "ffs_abi_version",
@@ -67,6 +67,18 @@ class Surface(C.Structure):
         ("vertices", C.c_void_p), ("velocities", C.c_void_p), ("elements", C.c_void_p),
         ("num_vertices", C.c_int), ("num_elements", C.c_int),
         ("forces", C.c_void_p), ("forces64", C.c_void_p),
+    ]
+
+
+class VolumeSurface(C.Structure):
+    """ffs_volume_surface: a surface given through its volume mesh's arrays and the
+    surface-to-volume vertex map."""
+    _fields_ = [
+        ("dim", C.c_int), ("num_volume_vertices", C.c_int),
+        ("volume_positions", C.c_void_p), ("volume_velocities", C.c_void_p), ("volume_forces", C.c_void_p),
+        ("num_vertices", C.c_int), ("num_elements", C.c_int),
+        ("surface_to_volume", C.c_void_p), ("elements", C.c_void_p),
+        ("surface_positions", C.c_void_p), ("surface_velocities", C.c_void_p),
     ]
 
 
@@ -130,6 +142,7 @@ def load():
         "ffs_lbm_reserve_surface": [vp, i32, i32],
         "ffs_lbm_step": [vp, C.POINTER(Surface), vp],
         "ffs_lbm_step_noalloc": [vp, C.POINTER(Surface), vp],
+        "ffs_lbm_step_coupled": [vp, C.POINTER(VolumeSurface), vp],
         "ffs_lbm_fill_solid": [vp, C.POINTER(Surface), vp],
         "ffs_lbm_get_status": [vp, C.POINTER(C.c_uint32), i32, vp],
         "ffs_lbm_get_info": [vp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i32), C.POINTER(C.c_double),

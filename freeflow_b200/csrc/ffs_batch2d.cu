@@ -54,7 +54,7 @@ template <typename T> __device__ __forceinline__ GridArgs<T> episode_args(const 
 
 __device__ __forceinline__ SurfaceArgs episode_surface(const PoolEpisode &e)
 {
-    SurfaceArgs s;
+    SurfaceArgs s{};
     s.V = e.V;
     s.U = e.U;
     s.E = e.elements;

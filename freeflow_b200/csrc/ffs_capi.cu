@@ -146,10 +146,10 @@ ffs_status ensure_links(ffs_lbm *h, int64_t max_vertices, int64_t max_link_cells
 
 // link cells a surface can own at most: every element's grown bounding box,
 // bounded by the grid; a generous default for the on-demand path
-int64_t default_link_cells(const ffs_lbm *h, const ffs_surface *s)
+int64_t default_link_cells(const ffs_lbm *h, int64_t num_elements)
 {
     int64_t per = h->dim == 2 ? 12 : 40;
-    return std::min<int64_t>((int64_t)s->num_elements * per + 4096, h->ncell);
+    return std::min<int64_t>(num_elements * per + 4096, h->ncell);
 }
 
 ffs_status check_surface(const ffs_lbm *h, const ffs_surface *s)
@@ -210,18 +210,17 @@ struct StageTimer {
     }
 };
 
-template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const ffs_surface *s, cudaStream_t st)
+template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const SurfaceArgs &sa, cudaStream_t st)
 {
     GridArgs<T> g = args<T>(h);
-    const bool surf = s && s->num_elements > 0;
-    SurfaceArgs sa = surface_args(s);
+    const bool surf = sa.ne > 0;
     StepScalars sc{h->cl, h->ct, h->cf};
     uint32_t *words = reinterpret_cast<uint32_t *>(h->flags);
     if (DIM == 3 && h->dense_variant < 0) h->dense_variant = tune_dense3d<T>(g, st);
     if (surf) {
-        if (h->lt.cap == 0 || (int64_t)h->lt.acc_cap < s->num_vertices) {
-            ffs_status r = ensure_links(h, std::max<int64_t>(s->num_vertices, h->lt.acc_cap),
-                                        std::max<int64_t>(default_link_cells(h, s), h->lt.cap / 2));
+        if (h->lt.cap == 0 || (int64_t)h->lt.acc_cap < sa.nv) {
+            ffs_status r = ensure_links(h, std::max<int64_t>(sa.nv, h->lt.acc_cap),
+                                        std::max<int64_t>(default_link_cells(h, sa.ne), h->lt.cap / 2));
             if (r != FFS_OK) return r;
         }
         // Link detection and the dense pass overlap: the dense pass skips
@@ -253,12 +252,12 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const ffs_surfac
     return FFS_OK;
 }
 
-template <int DIM> ffs_status step_dim(ffs_lbm *h, const ffs_surface *s, cudaStream_t st)
+template <int DIM> ffs_status step_dim(ffs_lbm *h, const SurfaceArgs &sa, cudaStream_t st)
 {
     switch (h->d.storage) {
-    case FFS_STORAGE_F32: return step_impl<DIM, float>(h, s, st);
-    case FFS_STORAGE_F16: return step_impl<DIM, __half>(h, s, st);
-    default: return step_impl<DIM, __nv_bfloat16>(h, s, st);
+    case FFS_STORAGE_F32: return step_impl<DIM, float>(h, sa, st);
+    case FFS_STORAGE_F16: return step_impl<DIM, __half>(h, sa, st);
+    default: return step_impl<DIM, __nv_bfloat16>(h, sa, st);
     }
 }
 
@@ -547,7 +546,32 @@ ffs_status ffs_lbm_step(ffs_lbm *h, const ffs_surface *s, void *stream)
     if (!h) return fail(FFS_ERR_INVALID_ARGUMENT, "null grid");
     ffs_status r = check_surface(h, s);
     if (r != FFS_OK) return r;
-    return h->dim == 2 ? step_dim<2>(h, s, S(stream)) : step_dim<3>(h, s, S(stream));
+    const SurfaceArgs sa = surface_args(s);
+    return h->dim == 2 ? step_dim<2>(h, sa, S(stream)) : step_dim<3>(h, sa, S(stream));
+}
+
+ffs_status ffs_lbm_step_coupled(ffs_lbm *h, const ffs_volume_surface *s, void *stream)
+{
+    if (!h || !s) return fail(FFS_ERR_INVALID_ARGUMENT, "null argument");
+    if (s->dim != h->dim) return fail(FFS_ERR_INVALID_ARGUMENT, "surface dim differs from grid dim");
+    if (s->num_vertices < 0 || s->num_elements < 0 || s->num_volume_vertices < 0)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "negative surface size");
+    if (s->num_vertices > 0 && (!s->volume_positions || !s->volume_velocities || !s->surface_to_volume ||
+                                !s->surface_positions || !s->surface_velocities))
+        return fail(FFS_ERR_INVALID_ARGUMENT, "surface arrays must be device pointers");
+    if (s->num_elements > 0 && (!s->elements || s->num_vertices <= 0))
+        return fail(FFS_ERR_INVALID_ARGUMENT, "surface has elements but no vertices");
+    if (s->num_volume_vertices > 0 && !s->volume_forces)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "volume_forces must be a device pointer");
+    cudaStream_t st = S(stream);
+    FFS_CK(launch_gather_surface(h->dim, s->volume_positions, s->volume_velocities, s->surface_to_volume,
+                                 s->num_vertices, s->num_volume_vertices, s->surface_positions, s->surface_velocities,
+                                 s->volume_forces, h->status, st));
+    SurfaceArgs sa{};
+    sa.V = s->surface_positions; sa.U = s->surface_velocities; sa.E = s->elements;
+    sa.nv = s->num_vertices; sa.ne = s->num_elements;
+    sa.map = s->surface_to_volume; sa.vforces = s->volume_forces; sa.nvol = s->num_volume_vertices;
+    return h->dim == 2 ? step_dim<2>(h, sa, st) : step_dim<3>(h, sa, st);
 }
 
 ffs_status ffs_lbm_fill_solid(ffs_lbm *h, const ffs_surface *s, void *stream)
@@ -600,7 +624,7 @@ ffs_status ffs_lbm_debug_links(ffs_lbm *h, const ffs_surface *s, uint64_t *cell_
     if (s->num_elements == 0) return FFS_OK;
     cudaStream_t st = S(stream);
     r = ensure_links(h, std::max<int64_t>(s->num_vertices, h->lt.acc_cap),
-                     std::max<int64_t>(default_link_cells(h, s), h->lt.cap / 2));
+                     std::max<int64_t>(default_link_cells(h, s->num_elements), h->lt.cap / 2));
     if (r != FFS_OK) return r;
     SurfaceArgs sa = surface_args(s);
     StepScalars sc{h->cl, h->ct, h->cf};

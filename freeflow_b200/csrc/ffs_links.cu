@@ -184,6 +184,10 @@ __global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint3
     }
 }
 
+// Fixed-point sums -> physical forces: added to the surface's force arrays,
+// or, in the coupled step, written to the mapped volume vertices (whose
+// forces the gather zeroed), as scatterSurfaceForcesToVolume assigns them
+// (src/fsi/FsiCouplingKernels.cu:59-90).
 template <int DIM>
 __global__ void finalize_forces_kernel(LinkTable lt, SurfaceArgs s, double cf)
 {
@@ -192,12 +196,46 @@ __global__ void finalize_forces_kernel(LinkTable lt, SurfaceArgs s, double cf)
         long long a = lt.acc[t];
         if (a != 0) {
             double f = (double)a * (1.0 / kForceScale) * cf;
-            if (s.forces) s.forces[t] += (float)f;
-            if (s.forces64) s.forces64[t] += f;
+            if (s.vforces) {
+                const long long i = t / DIM;
+                const uint32_t m = s.map[i];
+                if (m < (uint32_t)s.nvol) s.vforces[(size_t)m * DIM + (t - i * DIM)] = (float)f;
+            } else {
+                if (s.forces) s.forces[t] += (float)f;
+                if (s.forces64) s.forces64[t] += f;
+            }
             lt.acc[t] = 0;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *lt.count = 0;
+}
+
+// First stage of the coupled step (updateSurfaceStatesFromVolume,
+// src/fsi/FsiCouplingKernels.cu:14-57, plus the volume-force zeroing of the
+// solid solver's applyForces, src/fem/VBDSolver.cpp:105,289).  Map entries
+// out of range latch the element-index status bit and gather zeros.
+template <int DIM>
+__global__ void gather_surface_kernel(const float *vpos, const float *vvel, const uint32_t *map, int nv, int nvol,
+                                      float *spos, float *svel, float *vforces, uint32_t *status)
+{
+    const long long ns = (long long)nv * DIM, nz = (long long)nvol * DIM;
+    const long long n = ns > nz ? ns : nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        if (t < nz) vforces[t] = 0.0f;
+        if (t < ns) {
+            const long long i = t / DIM;
+            const uint32_t m = map[i];
+            float p = 0.0f, u = 0.0f;
+            if (m < (uint32_t)nvol) {
+                p = vpos[(size_t)m * DIM + (t - i * DIM)];
+                u = vvel[(size_t)m * DIM + (t - i * DIM)];
+            } else {
+                atomicOr(status, kStatusBadElement);
+            }
+            spos[t] = p;
+            svel[t] = u;
+        }
+    }
 }
 
 template <int DIM>
@@ -257,6 +295,17 @@ cudaError_t launch_finalize_forces(const LinkTable &lt, const SurfaceArgs &s, do
     int grid = (int)std::min<long long>((n + 255) / 256, (long long)sm_count() * 8);
     if (grid < 1) grid = 1;
     finalize_forces_kernel<DIM><<<grid, 256, 0, st>>>(lt, s, cf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_surface(int dim, const float *vpos, const float *vvel, const uint32_t *map, int nv, int nvol,
+                                  float *spos, float *svel, float *vforces, uint32_t *status, cudaStream_t st)
+{
+    const long long n = (long long)std::max(nv, nvol) * dim;
+    if (n == 0) return cudaSuccess;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)sm_count() * 8));
+    if (dim == 2) gather_surface_kernel<2><<<grid, 256, 0, st>>>(vpos, vvel, map, nv, nvol, spos, svel, vforces, status);
+    else gather_surface_kernel<3><<<grid, 256, 0, st>>>(vpos, vvel, map, nv, nvol, spos, svel, vforces, status);
     return cudaGetLastError();
 }
 

@@ -28,6 +28,11 @@ struct SurfaceArgs {
     int nv, ne;
     float *forces;
     double *forces64;
+    // coupled step: the surface is the boundary of a volume mesh; the step's
+    // forces are written to vforces[map[i]] (nvol volume vertices) instead
+    const uint32_t *map = nullptr;
+    float *vforces = nullptr;
+    int nvol = 0;
 };
 
 struct StepScalars {
@@ -49,6 +54,10 @@ template <int DIM>
 cudaError_t launch_finalize_forces(const LinkTable &lt, const SurfaceArgs &s, double cf, cudaStream_t st);
 template <int DIM>
 cudaError_t launch_reset_links(const LinkTable &lt, uint32_t *flag_words, cudaStream_t st);
+// first stage of the coupled step: gathers the surface from the volume
+// arrays through the map and zeroes the volume forces
+cudaError_t launch_gather_surface(int dim, const float *vpos, const float *vvel, const uint32_t *map, int nv, int nvol,
+                                  float *spos, float *svel, float *vforces, uint32_t *status, cudaStream_t st);
 
 template <int DIM>
 cudaError_t launch_prepare_flags(uint8_t *flags, uint32_t *wallmask, int nx, int ny, int nz, cudaStream_t st);

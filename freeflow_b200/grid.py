@@ -86,6 +86,60 @@ class DeviceSurface:
         return s
 
 
+class VolumeSurface:
+    """A surface given as the boundary of a solid's volume mesh (the reference's
+    FsiCouplingDataGpu view): the solid's vertex arrays on the device plus the
+    surface-to-volume vertex map, for :meth:`FluidGrid.step_coupled`.
+
+    volume_positions / volume_velocities: (nvol, dim) float32, physical units;
+    surface_to_volume: (nv,) volume index of each surface vertex; elements:
+    (ne, dim) surface-vertex indices.  After each coupled step
+    ``volume_forces`` (nvol, dim) holds that step's fluid force at the mapped
+    vertices and zero elsewhere; ``surface_positions`` / ``surface_velocities``
+    hold the gathered surface.
+    """
+
+    def __init__(self, volume_positions, volume_velocities, surface_to_volume, elements, device="cuda"):
+        import torch
+
+        vp = np.ascontiguousarray(volume_positions, dtype=np.float32)
+        self.dim = int(vp.shape[1])
+        self.volume_positions = torch.as_tensor(vp, device=device).contiguous()
+        self.volume_velocities = torch.as_tensor(np.ascontiguousarray(volume_velocities, dtype=np.float32),
+                                                 device=device).contiguous()
+        assert self.volume_velocities.shape == self.volume_positions.shape
+        self.volume_forces = torch.zeros_like(self.volume_positions)
+        m = np.ascontiguousarray(surface_to_volume, dtype=np.uint32).reshape(-1)
+        self.surface_to_volume = torch.as_tensor(m.view(np.int32), device=device).contiguous()
+        e = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1, self.dim)
+        self.elements = torch.as_tensor(e.view(np.int32), device=device).contiguous()
+        self.surface_positions = torch.zeros((m.size, self.dim), dtype=torch.float32, device=device)
+        self.surface_velocities = torch.zeros_like(self.surface_positions)
+
+    def update(self, volume_positions=None, volume_velocities=None):
+        import torch
+
+        for dst, a in ((self.volume_positions, volume_positions), (self.volume_velocities, volume_velocities)):
+            if a is not None:
+                dst.copy_(a.to(dst.device, torch.float32) if isinstance(a, torch.Tensor)
+                          else torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32)))
+
+    def c_struct(self) -> A.VolumeSurface:
+        s = A.VolumeSurface()
+        s.dim = self.dim
+        s.num_volume_vertices = int(self.volume_positions.shape[0])
+        s.volume_positions = self.volume_positions.data_ptr()
+        s.volume_velocities = self.volume_velocities.data_ptr()
+        s.volume_forces = self.volume_forces.data_ptr()
+        s.num_vertices = int(self.surface_to_volume.shape[0])
+        s.num_elements = int(self.elements.shape[0])
+        s.surface_to_volume = self.surface_to_volume.data_ptr()
+        s.elements = self.elements.data_ptr()
+        s.surface_positions = self.surface_positions.data_ptr()
+        s.surface_velocities = self.surface_velocities.data_ptr()
+        return s
+
+
 @dataclass
 class GridInfo:
     ncell: int
@@ -183,6 +237,12 @@ class FluidGrid:
     def step(self, surface: DeviceSurface | None = None, stream=None):
         s = surface.c_struct() if surface is not None else None
         A.check(A.load().ffs_lbm_step(self._h, C.byref(s) if s is not None else None, _stream_handle(stream)), "step")
+
+    def step_coupled(self, surface: VolumeSurface, stream=None):
+        """One coupled step (ffs_lbm_step_coupled): gather the surface from the volume mesh,
+        step the fluid, write this step's forces to ``surface.volume_forces``."""
+        s = surface.c_struct()
+        A.check(A.load().ffs_lbm_step_coupled(self._h, C.byref(s), _stream_handle(stream)), "step_coupled")
 
     def fill_solid(self, surface: DeviceSurface, stream=None):
         s = surface.c_struct()

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 2
+#define FFS_ABI_VERSION 3
 
 typedef struct ffs_lbm ffs_lbm;
 
@@ -97,6 +97,33 @@ typedef struct {
     double *forces64;
 } ffs_surface;
 
+/* A surface given as the boundary of a solid's volume mesh: the solid's own
+ * vertex arrays plus the surface-to-volume vertex map, as
+ * FsiCouplingDataGpu holds them (include/FSI_Simulator/fsi/
+ * FsiCouplingDataGpu.cuh:18-30).  All pointers are DEVICE pointers;
+ * positions, velocities and forces are DIM floats per vertex.
+ *   volume_positions/velocities  the solid's vertices (physical units)
+ *   volume_forces                output, see ffs_lbm_step_coupled
+ *   surface_to_volume[i]         volume index of surface vertex i
+ *   elements                     DIM surface-vertex indices per element
+ *   surface_positions/velocities caller-owned arrays of num_vertices
+ *                                entries (FsiCouplingDataGpu::
+ *                                surface_positions/velocities); the step
+ *                                writes the gathered surface there. */
+typedef struct {
+    int dim;
+    int num_volume_vertices;
+    const float *volume_positions;
+    const float *volume_velocities;
+    float *volume_forces;
+    int num_vertices;
+    int num_elements;
+    const uint32_t *surface_to_volume;
+    const uint32_t *elements;
+    float *surface_positions;
+    float *surface_velocities;
+} ffs_volume_surface;
+
 /* Replaces the LbmFlowField2D/3D constructors (LbmFlowField2D.cpp:17-40,
  * LbmFlowField3D.cpp:18-41).  All cells start as Fluid with zero moments;
  * call ffs_lbm_set_flags + ffs_lbm_initialize next. */
@@ -139,6 +166,24 @@ ffs_status ffs_lbm_reserve_surface(ffs_lbm *grid, int max_vertices, int max_link
  * outlet update, and the buffer swap.  `surface` may be NULL (no solid).
  * Asynchronous on `stream`; no host synchronisation. */
 ffs_status ffs_lbm_step(ffs_lbm *grid, const ffs_surface *surface, void *stream);
+
+/* One coupled fluid step as Simulator2D/3D::step runs it (src/core/
+ * Simulator2D.cpp:93-107, Simulator3D.cpp:90-101), in one stream and with no
+ * host synchronisation:
+ *   1. the surface gather of FemScene2D/3D::getSurfaceProxyForFSI
+ *      (src/fem/FemScene.cpp:591-605, 1251-1264; updateSurfaceStatesFromVolume,
+ *      src/fsi/FsiCouplingKernels.cu:14-57, 93-131): surface_positions/
+ *      velocities[i] = volume_positions/velocities[surface_to_volume[i]];
+ *   2. the fluid step of ffs_lbm_step on that surface;
+ *   3. the solid solver's applyForces (src/fem/VBDSolver.cpp:101-113,
+ *      282-297; scatterSurfaceForcesToVolume, FsiCouplingKernels.cu:59-90,
+ *      133-178): volume_forces is zeroed, then holds this step's fluid force
+ *      (Cf-scaled, physical units) at every mapped volume vertex.
+ * The reference synchronises after the gather (on stream 0) and after the
+ * scatter; here the three stages are kernels on `stream` and the call can be
+ * captured in a CUDA graph (every pointer is read at launch).  A map entry
+ * >= num_volume_vertices latches status bit 8 and that vertex is skipped. */
+ffs_status ffs_lbm_step_coupled(ffs_lbm *grid, const ffs_volume_surface *surface, void *stream);
 
 /* No counterpart in the reference.  The same step as ffs_lbm_step, with the
  * same results, but it allocates no device memory: its link table and force
