@@ -192,8 +192,10 @@ template <typename V> struct Coef3V {
     }
     // Evaluates the 27 populations slice by slice and hands each one to
     // sink(kz, ky, kx, value) as soon as it exists (k = c + 1), which keeps
-    // register pressure low when the sink stores to shared memory.
-    template <typename Sink> __device__ __forceinline__ void populations_each(Sink &&sink) const
+    // register pressure low when the sink stores to shared memory.  With
+    // WEIGHTED = false the values are the Hermite sums without their lattice
+    // weights (the caller applies the weights).
+    template <bool WEIGHTED = true, typename Sink> __device__ __forceinline__ void populations_each(Sink &&sink) const
     {
         V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
         herm3v(rho, m1z, m2zz, B00);
@@ -213,7 +215,10 @@ template <typename V> struct Coef3V {
                 V F[3];
                 herm3v(C0[ky], C1[ky], C2[ky], F);
 #pragma unroll
-                for (int kx = 0; kx < 3; ++kx) sink(kz, ky, kx, vconst<V>(wgt3(kx, ky, kz)) * F[kx]);
+                for (int kx = 0; kx < 3; ++kx) {
+                    if constexpr (WEIGHTED) sink(kz, ky, kx, vconst<V>(wgt3(kx, ky, kz)) * F[kx]);
+                    else sink(kz, ky, kx, F[kx]);
+                }
             }
         }
     }

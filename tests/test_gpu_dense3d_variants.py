@@ -100,3 +100,28 @@ def test_odd_width(cuda, variant):
     gm, om, _, _, st = run_pair(wl, 4)
     assert st == 0
     assert max_abs(gm, om) <= 4e-6
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_tuned_variants_round_identically(cuda, monkeypatch, storage):
+    """The first step's timing chooses between variants 0 and 1, so both must
+    give the same bits (moments and surface forces, with walls, an inlet, an
+    outlet and a moving surface): the choice cannot change a result."""
+    import torch
+
+    from helpers import make_gpu
+
+    wl = W.swimmer_3d(nx=64, ny=32, nz=32, body_frac=0.4, nlat=16, nlon=24, seed=4)
+    out = []
+    for v in ("0", "1"):
+        monkeypatch.setenv("FFS_DENSE3D_VARIANT", v)
+        g, s = make_gpu(wl, storage)
+        for k in range(6):
+            s.update(*wl.surface_at(k))
+            g.step(s)
+        torch.cuda.synchronize()
+        assert g.status() == 0
+        out.append((g.get_moments(), s.forces64.cpu().numpy()))
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
