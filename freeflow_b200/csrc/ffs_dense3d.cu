@@ -10,7 +10,8 @@
 //
 //   * each plane is reconstructed once for its 34 x 10 xy halo: every thread
 //     reconstructs its own cell, and the first 84 threads one cell of the
-//     ring around the tile as well;
+//     ring around the tile as well (only the 9 populations it feeds into the
+//     tile, one kind of ring cell per warp);
 //   * the populations of plane p go to one of two shared-memory buffers
 //     (2 x 27 x 340 floats) and are consumed as soon as they exist: the
 //     c_z = -1 slice completes the raw moments of the cell below (plane p-1),
@@ -45,14 +46,16 @@ constexpr int kPlane = D3::kPlaneFloats;
 
 __device__ __forceinline__ int set_of(int kx, int ky, int kz) { return (kz * 3 + ky) * 3 + kx; }
 
-// halo index (hx, hy) of ring cell r: rows y0-1 and y0+8 (34 cells each),
-// then columns x0-1 and x0+32 (8 cells each)
+// halo index (hx, hy) of ring cell r, grouped so that each warp holds one
+// kind of ring cell: r < 32 the row y0-1 (hx 1..32), r < 64 the row y0+8
+// (hx 1..32), r < 74 the column x0-1 (hy 0..9, corners included), r < 84
+// the column x0+32
 __device__ __forceinline__ int ring_cell(int r)
 {
-    if (r < 2 * kHX) return (r < kHX) ? r : (kHalo - kHX) + (r - kHX);
-    int q = r - 2 * kHX; // 0..15
-    int hy = 1 + (q & 7);
-    return hy * kHX + ((q < 8) ? 0 : kHX - 1);
+    if (r < 32) return r + 1;
+    if (r < 64) return (kHalo - kHX) + (r - 31);
+    if (r < 74) return (r - 64) * kHX;
+    return (r - 74) * kHX + kHX - 1;
 }
 
 // raw-moment slot: {rho, jx, jy, jz, Pxx, Pyy, Pzz, Pxy, Pyz, Pxz}
@@ -290,9 +293,40 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         cf.make(m);
         cf.populations_each<false>([&](int kz, int ky, int kx, float v) { buf[set_of(kx, ky, kz) * kHalo + c] = v; });
     };
+    // A ring cell feeds the tile only the 9 populations that point into it:
+    // c_y = +1 from the row below (warp 0), c_y = -1 from the row above
+    // (warp 1), c_x = +-1 from the columns (warp 2).  Each warp runs one
+    // uniform path that evaluates (or, for a bounce-back cell, zeroes) just
+    // those; no other slot of a ring cell is ever read.
+    const int ring_kind = tid < 32 ? 0 : tid < 64 ? 1 : 2;
+    const float ring_sx = tid < 74 ? 1.0f : -1.0f;                 // columns: c_x of the fed populations
+    const int ring_kxo = (tid < 74 ? 2 : 0) * kHalo;               // their kx plane offset
+    auto recon_ring = [&](float *buf) {
+        const int c = c_ring;
+        if (is_bounce_back<3>(hB)) {
+#pragma unroll
+            for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (ring_kind == 0) buf[set_of(k, 2, kz) * kHalo + c] = 0.0f;
+                    else if (ring_kind == 1) buf[set_of(k, 0, kz) * kHalo + c] = 0.0f;
+                    else buf[set_of(0, k, kz) * kHalo + ring_kxo + c] = 0.0f;
+                }
+            return;
+        }
+        decode_moments<3, T>(mB, g.codec);
+        Coef3V<float> cf;
+        cf.make(mB);
+        if (ring_kind == 0)
+            cf.populations_row<2>([&](int kz, int kx, float v) { buf[set_of(kx, 2, kz) * kHalo + c] = v; });
+        else if (ring_kind == 1)
+            cf.populations_row<0>([&](int kz, int kx, float v) { buf[set_of(kx, 0, kz) * kHalo + c] = v; });
+        else
+            cf.populations_col(ring_sx, [&](int kz, int ky, float v) { buf[set_of(0, ky, kz) * kHalo + ring_kxo + c] = v; });
+    };
     auto recon_plane = [&](float *buf) {
         recon_cell(buf, mA, hA, c_own);
-        if (has_ring) recon_cell(buf, mB, hB, c_ring);
+        if (has_ring) recon_ring(buf);
     };
     auto flag_at = [&](int z) -> uint32_t {
         return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[cell_at(z)] : 0u;

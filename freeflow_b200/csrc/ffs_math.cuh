@@ -222,6 +222,60 @@ template <typename V> struct Coef3V {
             }
         }
     }
+    // Only the 9 unweighted populations with c_y = KY - 1 (what a halo row
+    // outside a tile feeds into it), as sink(kz, kx, value), each
+    // bit-identical to populations_each<false>'s.
+    template <int KY, typename Sink> __device__ __forceinline__ void populations_row(Sink &&sink) const
+    {
+        V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
+        herm3v(rho, m1z, m2zz, B00);
+        herm3v(m1x, m2xz, qxzz, B10);
+        herm3v(m1y, m2yz, qyzz, B01);
+        herm2v(m2xx, qxxz, B20);
+        herm2v(m2yy, qyyz, B02);
+        herm2v(m2xy, qxyz, B11);
+        // entry KY of herm3v / herm2v, with herm3v's operations
+        auto h3 = [](V a0, V a1, V a2) {
+            if constexpr (KY == 1) return vfma(vconst<V>(-0.5f), a2, a0);
+            else if constexpr (KY == 0) return (a0 + a2) - a1;
+            else return (a0 + a2) + a1;
+        };
+        auto h2 = [](V a0, V a1) {
+            if constexpr (KY == 1) return a0;
+            else if constexpr (KY == 0) return a0 - a1;
+            else return a0 + a1;
+        };
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            V F[3];
+            herm3v(h3(B00[kz], B01[kz], B02[kz]), h3(B10[kz], B11[kz], qxyy), h2(B20[kz], qxxy), F);
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) sink(kz, kx, F[kx]);
+        }
+    }
+    // Only the 9 unweighted populations with c_x = sx (+1 or -1, given at run
+    // time: what a halo column outside a tile feeds into it), as
+    // sink(kz, ky, value), each bit-identical to populations_each<false>'s
+    // (herm3v's outer entries are (a0 + a2) -+ a1 = fma(-+1, a1, a0 + a2)).
+    template <typename Sink> __device__ __forceinline__ void populations_col(V sx, Sink &&sink) const
+    {
+        V B00[3], B10[3], B01[3], B20[3], B02[3], B11[3];
+        herm3v(rho, m1z, m2zz, B00);
+        herm3v(m1x, m2xz, qxzz, B10);
+        herm3v(m1y, m2yz, qyzz, B01);
+        herm2v(m2xx, qxxz, B20);
+        herm2v(m2yy, qyyz, B02);
+        herm2v(m2xy, qxyz, B11);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            V C0[3], C1[3], C2[3];
+            herm3v(B00[kz], B01[kz], B02[kz], C0);
+            herm3v(B10[kz], B11[kz], qxyy, C1);
+            herm2v(B20[kz], qxxy, C2);
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) sink(kz, ky, vfma(sx, C1[ky], C0[ky] + C2[ky]));
+        }
+    }
 };
 
 // ------------------------------------------------------------ raw moments
