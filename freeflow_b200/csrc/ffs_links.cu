@@ -48,12 +48,19 @@ template <auto KERNEL> static int resident_grid(int threads)
     return sm_count() * per_sm;
 }
 
-// D3Q27: one warp per triangle.  The triangle's own geometry is evaluated
-// once (tri_pre); lanes stride over (bounding-box cell, direction) pairs.  A
-// conservative plane-distance test discards the pairs whose link segment
-// clearly does not reach the triangle's plane (|signed distance of the cell|
-// > |projection of the link| + a margin of 2e-3 cells, far above the float
-// rounding of either quantity); every remaining pair gets the exact test.
+// D3Q27: one warp per triangle, one lane per link direction (lanes 0..25 for
+// l = 1..26).  The triangle's own geometry is evaluated once (tri_pre), and so
+// is each lane's projected link length a = cl n.c_l and its reciprocal; the
+// warp then walks the bounding-box cells (x fastest, nested loops, no index
+// arithmetic), and the cell's signed distance to the plane,
+// s1 = n.(p - v0), costs one multiply-add per cell (its y/z part is formed
+// once per row).  A conservative prefilter discards the (cell, direction)
+// pairs whose link segment clearly misses: the plane is not reached (t = s1 / a
+// outside [0, 1] by more than a margin of 2e-3 cells, tested as s1 sign(a)
+// against [-margin, |a| + margin]) or the plane point lies outside the
+// triangle by more than 1% in barycentric terms.  Every remaining pair gets
+// the exact, explicitly rounded test, so the link set does not depend on
+// this enumeration (the table keeps the minimum key per cell and direction).
 template <typename T>
 __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt,
                                                             SurfaceArgs s, StepScalars sc)
@@ -63,6 +70,11 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const float cl = sc.cl;
     const float margin = 2e-3f * cl;
+    const bool act = lane < Q - 1;
+    const int l = act ? lane + 1 : 1;
+    int cx, cy, cz;
+    dir_vec<3>(l, cx, cy, cz);
+    const float ccx = (float)cx * cl, ccy = (float)cy * cl, ccz = (float)cz * cl;
     for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < s.ne; e += nwarps) {
         const uint32_t ia = s.E[3 * e], ib = s.E[3 * e + 1], ic = s.E[3 * e + 2];
         if (ia >= (uint32_t)s.nv || ib >= (uint32_t)s.nv || ic >= (uint32_t)s.nv) {
@@ -83,67 +95,54 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
                 if (bmax[k] < c) bmax[k] = c;
             }
         const int n3[3] = {g.nx, g.ny, g.nz};
-        int lo[3], ext[3];
+        int lo[3], hi[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             lo[k] = max(__float2int_rz(geom::dvd(bmin[k], cl)) - 1, 0);
-            int hi = min(__float2int_rz(geom::dvd(bmax[k], cl)) + 1, n3[k] - 1);
-            ext[k] = max(hi - lo[k] + 1, 0);
+            hi[k] = min(__float2int_rz(geom::dvd(bmax[k], cl)) + 1, n3[k] - 1);
         }
-        const long long items = (long long)ext[0] * ext[1] * ext[2] * (Q - 1);
-        if (items == 0) continue;
-        // item it = cell * 26 + (l - 1), cell = (i - lo0) + ext0 * ((j - lo1) + ext1 * (k - lo2)).
-        // A lane steps by 32 items = one cell and 6 directions, so the cell
-        // and direction are carried forward instead of divided out.
-        int l = lane % (Q - 1) + 1;
-        int ci = 0, cj = 0, ck = 0;
-        auto advance = [&](int dc) {
-            ci += dc;
-            while (ci >= ext[0]) { ci -= ext[0]; ++cj; }
-            while (cj >= ext[1]) { cj -= ext[1]; ++ck; }
-        };
-        advance(lane / (Q - 1));
-        for (long long it = lane; it < items; it += 32) {
-            if (it != lane) {
-                l += 32 - (Q - 1);
-                int dc = 1;
-                if (l > Q - 1) { l -= Q - 1; dc = 2; }
-                advance(dc);
+        // this lane's direction against the triangle's plane
+        const float a = cl * (tr.n[0] * cx + tr.n[1] * cy + tr.n[2] * cz);
+        const float fa = fabsf(a);
+        const bool reach = fa > margin;              // else: the link runs (nearly) parallel to the plane
+        const float sg = a > 0.0f ? 1.0f : -1.0f;
+        const float inv_a = reach ? __fdividef(1.0f, a) : 0.0f;
+        for (int k3 = lo[2]; k3 <= hi[2]; ++k3) {
+            const float pz = (float)k3 * cl - tr.v0[2];
+            for (int j = lo[1]; j <= hi[1]; ++j) {
+                const float py = (float)j * cl - tr.v0[1];
+                const float s_yz = tr.n[1] * py + tr.n[2] * pz;
+                for (int i = lo[0]; i <= hi[0]; ++i) {
+                    const float px = (float)i * cl - tr.v0[0];
+                    const float s1 = fmaf(tr.n[0], px, s_yz);
+                    bool cand;
+                    if (reach) {
+                        const float sa = sg * s1;
+                        cand = !(sa < -margin || sa > fa + margin);
+                        if (cand) {
+                            // plane point relative to v0: p1 - t c cl - v0
+                            const float t = s1 * inv_a;
+                            const float wx = px - t * ccx, wy = py - t * ccy, wz = pz - t * ccz;
+                            const float d20 = wx * tr.e1[0] + wy * tr.e1[1] + wz * tr.e1[2];
+                            const float d21 = wx * tr.e2[0] + wy * tr.e2[1] + wz * tr.e2[2];
+                            const float u = (tr.d11 * d20 - tr.d01 * d21) * inv_den;
+                            const float v = (tr.d00 * d21 - tr.d01 * d20) * inv_den;
+                            cand = !(u < -0.01f || v < -0.01f || u + v > 1.01f);
+                        }
+                    } else {
+                        cand = !(fabsf(s1) > 2.0f * margin);
+                    }
+                    if (!(act && cand)) continue;
+                    float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
+                    float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl),
+                                   geom::mul(geom::sub((float)j, (float)cy), cl),
+                                   geom::mul(geom::sub((float)k3, (float)cz), cl)};
+                    const geom::Hit h = geom::isect3_pre(tr, p1, p2);
+                    if (!h.hit) continue;
+                    const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
+                    insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status);
+                }
             }
-            const int i = lo[0] + ci, j = lo[1] + cj, k3 = lo[2] + ck;
-            int cx, cy, cz;
-            dir_vec<3>(l, cx, cy, cz);
-            // prefilter in ordinary (fast) float math; it only rejects clear
-            // misses: the plane is not reached (t = s1 / a outside [0, 1] by
-            // more than a margin of 2e-3 cells, tested as s1 sign(a) against
-            // [-margin, |a| + margin]) or the plane point lies outside the
-            // triangle by more than 1% in barycentric terms
-            const float px = (float)i * cl - tr.v0[0], py = (float)j * cl - tr.v0[1], pz = (float)k3 * cl - tr.v0[2];
-            const float s1 = tr.n[0] * px + tr.n[1] * py + tr.n[2] * pz;
-            const float a = cl * (tr.n[0] * cx + tr.n[1] * cy + tr.n[2] * cz);
-            const float fa = fabsf(a);
-            if (fa > margin) {
-                const float sa = a > 0.0f ? s1 : -s1;
-                if (sa < -margin || sa > fa + margin) continue;
-                const float t = __fdividef(s1, a);
-                // plane point relative to v0: p1 - t c cl - v0
-                const float tc = t * cl;
-                const float wx = px - tc * cx, wy = py - tc * cy, wz = pz - tc * cz;
-                const float d20 = wx * tr.e1[0] + wy * tr.e1[1] + wz * tr.e1[2];
-                const float d21 = wx * tr.e2[0] + wy * tr.e2[1] + wz * tr.e2[2];
-                const float u = (tr.d11 * d20 - tr.d01 * d21) * inv_den;
-                const float v = (tr.d00 * d21 - tr.d01 * d20) * inv_den;
-                if (u < -0.01f || v < -0.01f || u + v > 1.01f) continue;
-            } else if (fabsf(s1) > 2.0f * margin) {
-                continue; // link parallel to the plane and away from it
-            }
-            float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
-            float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl), geom::mul(geom::sub((float)j, (float)cy), cl),
-                           geom::mul(geom::sub((float)k3, (float)cz), cl)};
-            const geom::Hit h = geom::isect3_pre(tr, p1, p2);
-            if (!h.hit) continue;
-            const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
-            insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status);
         }
     }
 }
