@@ -3,7 +3,8 @@
  * Python, no torch): it creates a D2Q9 channel with a cylinder given as a
  * device surface, starts it in uniform flow, steps it, and checks the
  * density, the flow downstream, the status word and the drag on the
- * cylinder.  It is what a
+ * cylinder; then it steps the same cylinder as the surface of a volume mesh
+ * through the coupled entry point.  It is what a
  * C or C++ host (the reference's Simulator2D, a solver of another language
  * through its FFI) does with the library.
  *
@@ -127,6 +128,57 @@ int main(void)
     if (!(rho_min > 0.9 && rho_max < 1.1)) { fprintf(stderr, "density out of range\n"); return 1; }
     if (!(ux_mean > 0.0)) { fprintf(stderr, "no flow downstream\n"); return 1; }
     if (!(fx > 0.0)) { fprintf(stderr, "the flow should push the cylinder downstream\n"); return 1; }
+
+    /* The same cylinder as the surface of a "volume mesh" of 2 * nseg
+     * vertices (surface vertex i is volume vertex 2 i + 1; the even ones are
+     * interior and never reach the fluid), stepped with the coupled entry
+     * point: gather, fluid step and force scatter on one stream. */
+    float hvv[4 * 48], hvu[4 * 48] = {0};
+    unsigned int hmap[48];
+    for (int i = 0; i < nseg; ++i) {
+        hmap[i] = (unsigned)(2 * i + 1);
+        hvv[4 * i] = hvv[4 * i + 1] = 1.0e3f; /* interior vertex far outside the grid */
+        hvv[4 * i + 2] = hv[2 * i];
+        hvv[4 * i + 3] = hv[2 * i + 1];
+    }
+    float *dvv, *dvu, *dvf, *dsp, *dsu;
+    unsigned int *dmap;
+    if (cudaMalloc((void **)&dvv, sizeof hvv) || cudaMalloc((void **)&dvu, sizeof hvu) ||
+        cudaMalloc((void **)&dvf, sizeof hvv) || cudaMalloc((void **)&dsp, sizeof hv) ||
+        cudaMalloc((void **)&dsu, sizeof hv) || cudaMalloc((void **)&dmap, sizeof hmap)) {
+        fprintf(stderr, "cudaMalloc failed\n");
+        return 1;
+    }
+    cudaMemcpy(dvv, hvv, sizeof hvv, cudaMemcpyHostToDevice);
+    cudaMemcpy(dvu, hvu, sizeof hvu, cudaMemcpyHostToDevice);
+    cudaMemcpy(dmap, hmap, sizeof hmap, cudaMemcpyHostToDevice);
+    ffs_volume_surface vs = {0};
+    vs.dim = 2;
+    vs.num_volume_vertices = 2 * nseg;
+    vs.volume_positions = dvv;
+    vs.volume_velocities = dvu;
+    vs.volume_forces = dvf;
+    vs.num_vertices = nseg;
+    vs.num_elements = nseg;
+    vs.surface_to_volume = dmap;
+    vs.elements = de;
+    vs.surface_positions = dsp;
+    vs.surface_velocities = dsu;
+    for (int t = 0; t < 4; ++t) CHECK(ffs_lbm_step_coupled(g, &vs, NULL));
+    CHECK(ffs_lbm_get_status(g, &status, 1, NULL));
+    if (status) { fprintf(stderr, "device status %u after coupled steps\n", status); return 1; }
+    float hvf[4 * 48], hsp[2 * 48];
+    cudaMemcpy(hvf, dvf, sizeof hvf, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hsp, dsp, sizeof hsp, cudaMemcpyDeviceToHost);
+    double vfx = 0.0;
+    for (int i = 0; i < nseg; ++i) {
+        if (hvf[4 * i] != 0.0f || hvf[4 * i + 1] != 0.0f) { fprintf(stderr, "force on an interior vertex\n"); return 1; }
+        if (hsp[2 * i] != hv[2 * i] || hsp[2 * i + 1] != hv[2 * i + 1]) { fprintf(stderr, "gather mismatch\n"); return 1; }
+        vfx += hvf[4 * i + 2];
+    }
+    printf("coupled step: drag on the volume mesh %.6g\n", vfx);
+    if (!(vfx > 0.0)) { fprintf(stderr, "no drag scattered to the volume mesh\n"); return 1; }
+    cudaFree(dvv); cudaFree(dvu); cudaFree(dvf); cudaFree(dsp); cudaFree(dsu); cudaFree(dmap);
 
     CHECK(ffs_lbm_destroy(g));
     cudaFree(dv); cudaFree(du); cudaFree(de); cudaFree(dfrc);
