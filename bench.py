@@ -58,7 +58,7 @@ FALLBACK_HBM_GBS = 6650.0
 # cells it processes; the capture and its command are in the named profile.
 DENSE_TRAFFIC_PER_CELL = {
     (3, "f32"): (74.99, "profiles/dense3d_link_kernels_D3Q27_256x128x128_swimmer_f32.md"),
-    (3, "f16"): (35.41, "profiles/dense3d_D3Q27_256x128x128_swimmer_f16.md"),
+    (3, "f16"): (35.39, "profiles/dense3d_D3Q27_256x128x128_swimmer_f16.md"),
 }
 
 
