@@ -14,20 +14,29 @@ Existing configuration files and driver scripts therefore load and step unchange
 
 Scope is the fluid step.
 
+- Solids are read from Medit ``.mesh`` files (:mod:`freeflow_b200.meshio`) and kept as the
+  reference's ``FemScene`` keeps them: the vertices of all meshes, placed and concatenated in
+  mesh order (the volume mesh), its elements, and the surface that enters the fluid step (boundary
+  edges in 2D, boundary faces in 3D) with its surface-to-volume vertex map.
+- Each step is ``ffs_lbm_step_coupled``: the surface is gathered out of the volume vertices, the
+  fluid steps, and the fluid force of the step is written to the surface's volume vertices.
+- The accessors return what the reference's return (``ISolidSolver.hpp:49-105, 163-220``):
+  ``getVertices``, ``getVelocity`` and ``getForce`` the volume arrays, ``getTriangles`` /
+  ``getTetrahedra`` the volume elements, ``getBoundaryVertices``, ``getBoundaryElements`` and
+  ``getBoundaryPointIdx`` the surface, its elements and its vertex map.
 - The ``"static"`` solid solver is mirrored: a rigid body moved by ``apply_kinematic_control``
   (``src/fem/StaticBodySolver.cpp:122-151``).
-- The deformable solvers (``"vbd"``, Newton) are outside this package. A caller that owns a solid
-  model drives the surface with ``set_surface`` instead, the hook the reference's
-  ``SolidGeometryProxy_Device`` provides.
-- Solids are read from Medit ``.mesh`` files (:mod:`freeflow_b200.meshio`). Only their surface enters
-  the fluid step.
+- The deformable solvers (``"vbd"``, Newton) and LBS control are outside this package. A caller
+  that owns a solid model sets the volume vertices with ``set_surface`` instead.
 
-Two reference quirks are reachable here:
+Differences from the reference that a caller can see:
 
-- ``get_fluid_moments(buffer="A")`` returns buffer A as the reference does (``Simulator2D.hpp:41-43``).
-  The default returns the current buffer.
-- ``accumulate_forces=True`` keeps the static solver's never-zeroed force sums
-  (``StaticBodySolver.cpp:153-156``). By default, forces are those of the last step.
+- ``getForce`` holds the fluid force of the last step at the surface's volume vertices (zero
+  elsewhere), what ``applyForces`` writes for a deformable solver (``VBDSolver.cpp:101-113``). The
+  reference's static solver ignores the forces (``StaticBodySolver.cpp:153-156``), so its
+  ``getForce`` stays zero.
+- ``get_fluid_moments(buffer="A")`` returns buffer A as the reference does (``Simulator2D.hpp:41-43``);
+  the default returns the current buffer.
 """
 from __future__ import annotations
 
@@ -308,28 +317,64 @@ def flags_from_params(p) -> np.ndarray:
     return f.reshape(-1)
 
 
+# ----------------------------------------------------------------- solids
+@dataclass
+class SolidScene:
+    """The solids as FemScene holds them: volume vertices of all meshes (placed, concatenated in
+    mesh order), volume elements (triangles in 2D, tetrahedra in 3D) in volume numbering, the
+    surface elements in compact surface numbering, and each surface vertex's volume index."""
+    positions: np.ndarray          # (nvol, dim) float64
+    elements: np.ndarray           # (ne, dim + 1) int64
+    surface_elements: np.ndarray   # (ns, dim) uint32
+    surface_to_volume: np.ndarray  # (nsv,) uint32
+    mesh_of_vertex: np.ndarray     # (nvol,) int64
+
+
+def build_solid_scene(params, dim: int) -> SolidScene:
+    """Loads and places every solid of the configuration (FemScene2D/3D set-up)."""
+    pos, elems, surf, smap, owner = [], [], [], [], []
+    vbase = sbase = 0
+    for mid, s in enumerate(params.solids):
+        mesh = meshio.load_medit(s.mesh_path, dimension=dim)
+        v = meshio.place(mesh.vertices, s.translate, s.rotate, s.scale)
+        vol_el = mesh.triangles if dim == 2 else mesh.tetrahedra
+        _, se, ids = meshio.surface_of(mesh)
+        pos.append(v)
+        elems.append(vol_el.astype(np.int64) + vbase)
+        surf.append(se.astype(np.int64) + sbase)
+        smap.append(ids.astype(np.int64) + vbase)
+        owner.append(np.full(len(v), mid))
+        vbase += len(v)
+        sbase += len(ids)
+    if not pos:
+        z = np.zeros
+        return SolidScene(z((0, dim)), z((0, dim + 1), np.int64), z((0, dim), np.uint32), z(0, np.uint32),
+                          z(0, np.int64))
+    return SolidScene(np.concatenate(pos), np.concatenate(elems), np.concatenate(surf).astype(np.uint32),
+                      np.concatenate(smap).astype(np.uint32), np.concatenate(owner))
+
+
 # ------------------------------------------------------------- simulators
 class _SimulatorBase:
     DIM = 2
 
-    def __init__(self, params, storage: str = "f32", accumulate_forces: bool = False):
+    def __init__(self, params, storage: str = "f32"):
         self.m_params = params
         self.storage = storage
-        self.accumulate_forces = accumulate_forces
         self._grid = None
-        self._surf = None
+        self._vs = None
         self._fluid_enabled = True
         self._profile_name = None
         self._targets, self._vel, self._target_index = [], 0.0, -1
 
     # -- set-up
     def initialize(self):
-        from .grid import DeviceSurface, FluidGrid
+        from .grid import FluidGrid, VolumeSurface
 
         p = self.m_params
         if p.solid_solver_type not in ("static",):
             raise ValueError(f"solid_solver_type '{p.solid_solver_type}': only the static (kinematic) solid is part of "
-                             "this package; drive a deformable surface through set_surface()")
+                             "this package; drive a deformable solid through set_surface()")
         bc = list(p.boundary_velocities)
         if len(bc) != 2 * self.DIM:
             bc = [0.0] * (2 * self.DIM)
@@ -339,40 +384,29 @@ class _SimulatorBase:
         self._flags = flags_from_params(p)
         self._grid.set_flags(self._flags)
         self._grid.initialize()
-        verts, elems, self._mesh_of_vertex = [], [], []
-        base = 0
-        self._marker0 = None
-        for mid, s in enumerate(p.solids):
-            mesh = meshio.load_medit(s.mesh_path, dimension=self.DIM)
-            if mid == 0:  # the static solver's marker: the scene's first vertex
-                self._marker0 = meshio.place(mesh.vertices[:1], s.translate, s.rotate, s.scale)[0]
-            v, e, _ = meshio.surface_of(mesh)
-            v = meshio.place(v, s.translate, s.rotate, s.scale)
-            verts.append(v)
-            elems.append(e.astype(np.int64) + base)
-            self._mesh_of_vertex.append(np.full(len(v), mid))
-            base += len(v)
-        if verts:
-            self._rest = np.concatenate(verts).astype(np.float32)
-            self._elements = np.concatenate(elems).astype(np.uint32)
-            v0 = np.concatenate([np.tile(np.asarray(s.initial_velocity, np.float32), (len(v), 1))
-                                 for s, v in zip(p.solids, verts)])
-            self._surf = DeviceSurface(self._rest, v0, self._elements, with_forces64=True)
-            self._pos = self._rest.astype(np.float64)
-            self._vel_now = v0.astype(np.float64)
+        self._scene = build_solid_scene(p, self.DIM)
+        sc = self._scene
+        if len(sc.positions):
+            self._rest = sc.positions.copy()
+            self._vel0 = np.concatenate([np.tile(np.asarray(s.initial_velocity, np.float64)[:self.DIM],
+                                                 (int((sc.mesh_of_vertex == mid).sum()), 1))
+                                         for mid, s in enumerate(p.solids)])
+            self._pos = self._rest.copy()
+            self._vel_now = self._vel0.copy()
+            self._marker0 = self._rest[0].copy()   # the static solver's marker: the scene's first vertex
             self._marker = self._marker0.copy()
+            self._vs = VolumeSurface(self._pos, self._vel_now, sc.surface_to_volume, sc.surface_elements)
 
     def reset(self):
         if self._grid is not None:
             self._grid.set_flags(self._flags)
             self._grid.initialize()
-        if self._surf is not None:
-            self._pos = self._rest.astype(np.float64)
-            self._vel_now[:] = 0.0
+        if self._vs is not None:
+            self._pos = self._rest.copy()
+            self._vel_now = np.zeros_like(self._vel0)
             self._marker = self._marker0.copy()
-            self._surf.update(self._pos, self._vel_now)
-            self._surf.forces.zero_()
-            self._surf.forces64.zero_()
+            self._vs.update(self._pos, self._vel_now)
+            self._vs.volume_forces.zero_()
         self._targets, self._vel, self._target_index = [], 0.0, -1
 
     def enableFluidSolver(self, enable: bool):  # noqa: N802 -- reference name
@@ -381,18 +415,18 @@ class _SimulatorBase:
     # -- stepping (Simulator2D.cpp:88-130)
     def step(self):
         if self._fluid_enabled:
-            if self._surf is not None and not self.accumulate_forces:
-                self._surf.forces.zero_()
-                self._surf.forces64.zero_()
-            self._grid.step(self._surf)
+            if self._vs is not None:
+                self._grid.step_coupled(self._vs)
+            else:
+                self._grid.step()
         self._advance_solid()
 
     def set_surface(self, vertices, velocities):
-        """Positions and velocities of every surface vertex (physical units), for a caller that
-        owns the solid model; the surface's elements are fixed at initialize()."""
+        """Positions and velocities of every vertex of the solids' volume mesh (physical units), for
+        a caller that owns the solid model; the surface is gathered from them at every step."""
         self._pos = np.asarray(vertices, np.float64).reshape(-1, self.DIM)
         self._vel_now = np.asarray(velocities, np.float64).reshape(-1, self.DIM)
-        self._surf.update(self._pos, self._vel_now)
+        self._vs.update(self._pos, self._vel_now)
 
     def apply_kinematic_control(self, mesh_id: int, target_pos, vel: float):
         """StaticBodySolver::applyKinematicControl (StaticBodySolver.cpp:158-180): the body moves
@@ -411,8 +445,9 @@ class _SimulatorBase:
         self._target_index = -1
 
     def _advance_solid(self):
-        # StaticBodySolver2D/3D::advanceTimeStep (StaticBodySolver.cpp:122-151)
-        if not self._targets or self._vel <= 0.0 or self._surf is None:
+        # StaticBodySolver2D/3D::advanceTimeStep (StaticBodySolver.cpp:122-151): every vertex of
+        # the scene moves with the marker's velocity
+        if not self._targets or self._vel <= 0.0 or self._vs is None:
             return
         dt = self.m_params.dt
         marker = self._marker
@@ -427,7 +462,7 @@ class _SimulatorBase:
         self._vel_now[:] = v
         self._pos += v * dt
         self._marker = self._marker + v * dt
-        self._surf.update(self._pos, self._vel_now)
+        self._vs.update(self._pos, self._vel_now)
 
     # -- accessors (bindings.cpp:307-321)
     def get_fluid_moments(self, buffer: str = "current") -> np.ndarray:
@@ -439,21 +474,47 @@ class _SimulatorBase:
         shape = (p.fluid_ny, p.fluid_nx, 6) if self.DIM == 2 else (p.fluid_nz, p.fluid_ny, p.fluid_nx, 10)
         return m.reshape(shape)
 
-    def getVertices(self):  # noqa: N802
-        return self._pos.astype(np.float32).copy() if self._surf is not None else np.zeros((0, self.DIM), np.float32)
+    # ISolidSolver2D/3D accessors (ISolidSolver.hpp:49-105, 163-220)
+    def _none(self, width=None):
+        return np.zeros((0, width or self.DIM), np.float32)
 
-    getBoundaryVertices = getVertices
+    def getVertices(self):  # noqa: N802
+        """Positions of every vertex of the solids' volume mesh."""
+        return self._pos.astype(np.float32) if self._vs is not None else self._none()
 
     def getVelocity(self):  # noqa: N802
-        return self._vel_now.astype(np.float32).copy() if self._surf is not None else np.zeros((0, self.DIM), np.float32)
+        return self._vel_now.astype(np.float32) if self._vs is not None else self._none()
 
     def getForce(self):  # noqa: N802
-        if self._surf is None:
-            return np.zeros((0, self.DIM), np.float32)
-        return self._surf.forces.cpu().numpy()
+        """Fluid force of the last step on each volume vertex (zero off the surface)."""
+        return self._vs.volume_forces.cpu().numpy() if self._vs is not None else self._none()
+
+    def getBoundaryVertices(self):  # noqa: N802
+        """Positions of the surface vertices (the surface the fluid step sees)."""
+        if self._vs is None:
+            return self._none()
+        return self._pos[self._scene.surface_to_volume].astype(np.float32)
 
     def getBoundaryElements(self):  # noqa: N802
-        return self._elements.reshape(-1).copy() if self._surf is not None else np.zeros(0, np.uint32)
+        """Surface elements, flattened, in surface-vertex numbering."""
+        return self._scene.surface_elements.reshape(-1).copy() if self._vs is not None else np.zeros(0, np.uint32)
+
+    def getBoundaryPointIdx(self):  # noqa: N802
+        """Volume index of each surface vertex (the surface-to-volume map)."""
+        return self._scene.surface_to_volume.copy() if self._vs is not None else np.zeros(0, np.uint32)
+
+    def getControlPointIdx(self):  # noqa: N802
+        """LBS control points; LBS control is not part of this package, so there are none."""
+        return []
+
+    def getLBSVertices(self):  # noqa: N802
+        raise NotImplementedError("LBS control is not supported for the static solid solver")
+
+    def _surface_now(self):
+        from .grid import DeviceSurface
+
+        m = self._scene.surface_to_volume
+        return DeviceSurface(self._pos[m], self._vel_now[m], self._scene.surface_elements)
 
     def status(self) -> int:
         """Device status bits (non-finite state, link overflow, force range, bad element); clears them."""
@@ -465,7 +526,8 @@ class _SimulatorBase:
         os.makedirs(self.m_params.output_path, exist_ok=True)
         np.savez(os.path.join(self.m_params.output_path, f"frame_{int(frame_index):06d}.npz"),
                  moments=self.get_fluid_moments(), vertices=self.getVertices(), velocities=self.getVelocity(),
-                 forces=self.getForce())
+                 forces=self.getForce(), boundary_elements=self.getBoundaryElements(),
+                 boundary_point_idx=self.getBoundaryPointIdx())
 
     def begin_profiler(self, name: str):
         """Starts per-stage CUDA-event timing of the steps (detect, dense, link cells, forces)."""
@@ -490,10 +552,14 @@ class _SimulatorBase:
 class Simulator2D(_SimulatorBase):
     DIM = 2
 
+    def getTriangles(self):  # noqa: N802
+        """Triangles of the solids' volume mesh, flattened, in volume numbering."""
+        return self._scene.elements.reshape(-1).astype(np.uint32) if self._vs is not None else np.zeros(0, np.uint32)
+
     def fill_solid(self):
         """fillSolidFlags2D (FsiCoupling2D.cu:434-464): fluid cells inside the solid become
         SolidDynamic; returns their [x, y] list (Simulator2D.cpp:132-151)."""
-        self._grid.fill_solid(self._surf)
+        self._grid.fill_solid(self._surface_now())
         f = self._grid.get_flags()
         idx = np.nonzero(f == SOLID_DYNAMIC)[0]
         return [[int(i % self.m_params.fluid_nx), int(i // self.m_params.fluid_nx)] for i in idx]
@@ -503,3 +569,8 @@ class Simulator2D(_SimulatorBase):
 
 class Simulator3D(_SimulatorBase):
     DIM = 3
+
+    def getTetrahedra(self):  # noqa: N802
+        """Tetrahedra of the solids' volume mesh, flattened, in volume numbering (none for a
+        solid given as a surface mesh)."""
+        return self._scene.elements.reshape(-1).astype(np.uint32) if self._vs is not None else np.zeros(0, np.uint32)

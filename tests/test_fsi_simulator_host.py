@@ -158,3 +158,34 @@ def test_place_follows_the_reference_conventions():
     assert np.allclose(r, [[1.0, 0.0, 0.0]], atol=1e-12)
     assert math.isclose(np.linalg.norm(meshio.place(np.array([[3.0, 4.0, 0.0]]), [0, 0, 0], [10, 20, 30],
                                                     [1, 1, 1])), 5.0)
+
+
+def test_solid_scene_volume_surface_and_map(tmp_path):
+    """Two solids become one scene as FemScene builds it: volume vertices placed and
+    concatenated in mesh order, volume triangles in volume numbering, surface edges
+    in compact surface numbering, and a map from surface to volume vertices whose
+    positions are the surface's."""
+    v, t = _square_mesh(3)                      # 16 vertices, 4 interior, 18 triangles
+    a, b = str(tmp_path / "a.mesh"), str(tmp_path / "b.mesh")
+    meshio.write_medit(a, v, triangles=t)
+    meshio.write_medit(b, v, triangles=t)
+    p = F.SimulationParameters2D(fluid_nx=32, fluid_ny=16)
+    p.solids = [F.SolidBodyConfig2D(mesh_path=a, translate=[0.1, 0.2], scale=[0.5, 0.5], rotate=0.0),
+                F.SolidBodyConfig2D(mesh_path=b, translate=[0.6, 0.2], scale=[0.25, 0.25], rotate=30.0)]
+    sc = F.build_solid_scene(p, 2)
+    assert sc.positions.shape == (32, 2) and sc.elements.shape == (36, 3)
+    assert np.array_equal(sc.elements[18:], t + 16)
+    assert np.allclose(sc.positions[:16], meshio.place(v, [0.1, 0.2], 0.0, [0.5, 0.5]))
+    assert np.allclose(sc.positions[16:], meshio.place(v, [0.6, 0.2], 30.0, [0.25, 0.25]))
+    assert sc.surface_to_volume.size == 24 and sc.surface_elements.shape == (24, 2)
+    interior = {5, 6, 9, 10}
+    assert not (set(sc.surface_to_volume[:12].tolist()) & interior)
+    assert not (set((sc.surface_to_volume[12:] - 16).tolist()) & interior)
+    # surface elements of the second solid use surface indices 12..23 and map into its vertices
+    assert sc.surface_elements[:12].max() < 12 and sc.surface_elements[12:].min() >= 12
+    assert (sc.surface_to_volume[sc.surface_elements[12:]] >= 16).all()
+    # each surface edge is an edge of a volume triangle
+    tri_edges = {tuple(sorted(e)) for tr in sc.elements for e in ((tr[0], tr[1]), (tr[1], tr[2]), (tr[2], tr[0]))}
+    for e in sc.surface_to_volume[sc.surface_elements]:
+        assert tuple(sorted(e.tolist())) in tri_edges
+    assert np.array_equal(sc.mesh_of_vertex, np.repeat([0, 1], 16))

@@ -1,7 +1,10 @@
 """The fsi_simulator mirror on the GPU: a JSON configuration and a Medit mesh
 in the reference's formats drive Simulator2D / Simulator3D, and the steps
 match the oracle fed the same surfaces (tolerances of test_gpu_parity.py:
-moments 2e-6, forces 1e-4 x max |F|)."""
+moments 2e-6, forces 1e-4 x max |F|).  The accessors return the volume mesh
+as the reference's do: the surface is getBoundaryVertices / getBoundaryElements
+with the map getBoundaryPointIdx, and getForce holds the last step's force on
+the surface's volume vertices."""
 import json
 import math
 
@@ -61,15 +64,22 @@ def test_simulator2d_config_mesh_and_kinematic_body_match_oracle(cuda, tmp_path)
     o = _oracle_for(sim, p, 2)
     elements = sim.getBoundaryElements().reshape(-1, 2)
     assert elements.shape == (40, 2)
+    # the volume mesh is the disk fan: its centre vertex is interior
+    smap = sim.getBoundaryPointIdx()
+    assert sim.getVertices().shape == (41, 2) and sim.getTriangles().size == 40 * 3
+    assert smap.size == 40 and 0 not in smap
+    assert np.array_equal(sim.getBoundaryVertices(), sim.getVertices()[smap])
     for _ in range(6):
-        V, U = sim.getVertices(), sim.getVelocity()
+        V, U = sim.getBoundaryVertices(), sim.getVelocity()[smap]
         Fo = np.zeros(V.size)
         o.step(V, U, elements, Fo)
         sim.step()
     assert max_abs(sim.get_fluid_moments().reshape(-1, 6), o.get_moments()) <= 2e-6
-    Fg = sim.getForce().reshape(-1).astype(np.float64)
+    F_all = sim.getForce()
+    Fg = F_all[smap].reshape(-1).astype(np.float64)
     assert np.abs(Fo).max() > 0
     assert max_abs(Fg, Fo) <= 1e-4 * np.abs(Fo).max() + 1e-6 * np.abs(Fg).max()
+    assert not F_all[0].any()       # no fluid force on the interior vertex
     # the body moved towards its first target at 0.02 per unit time
     assert np.allclose(sim.getVelocity()[0], 0.02 * np.array([0.2, 0.06]) / np.hypot(0.2, 0.06), rtol=1e-5)
     assert sim.status() == 0
@@ -120,13 +130,15 @@ def test_simulator3d_config_and_tet_mesh_match_oracle(cuda, tmp_path):
     o = _oracle_for(sim, p, 3)
     elements = sim.getBoundaryElements().reshape(-1, 3)
     assert elements.shape == (12, 3)
+    smap = sim.getBoundaryPointIdx()
+    assert sim.getVertices().shape == (8, 3) and sim.getTetrahedra().size == 6 * 4
     for _ in range(4):
-        V, U = sim.getVertices(), sim.getVelocity()
+        V, U = sim.getBoundaryVertices(), sim.getVelocity()[smap]
         Fo = np.zeros(V.size)
         o.step(V, U, elements, Fo)
         sim.step()
     assert max_abs(sim.get_fluid_moments().reshape(-1, 10), o.get_moments()) <= 4e-6
-    Fg = sim.getForce().reshape(-1).astype(np.float64)
+    Fg = sim.getForce()[smap].reshape(-1).astype(np.float64)
     assert np.abs(Fo).max() > 0
     assert max_abs(Fg, Fo) <= 1e-4 * np.abs(Fo).max() + 1e-6 * np.abs(Fg).max()
     o.close()
