@@ -510,6 +510,17 @@ class _SimulatorBase:
     def getLBSVertices(self):  # noqa: N802
         raise NotImplementedError("LBS control is not supported for the static solid solver")
 
+    # solid-model controls of the reference that belong to the deformable solvers
+    def apply_lbs_control(self, *args, **kwargs):
+        """Simulator2D/3D::applyLBSControl (LBS control of a deformable solid): not part of the
+        fluid step; a caller with its own solid model sets the vertices with set_surface()."""
+        raise NotImplementedError("LBS control belongs to the deformable solid solvers, outside this package")
+
+    def apply_active_strain(self, *args, **kwargs):
+        """Simulator2D::applyActiveStrain (active strain of a deformable solid): not part of the
+        fluid step."""
+        raise NotImplementedError("active strain belongs to the deformable solid solvers, outside this package")
+
     def _surface_now(self):
         from .grid import DeviceSurface
 

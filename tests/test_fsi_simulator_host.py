@@ -189,3 +189,17 @@ def test_solid_scene_volume_surface_and_map(tmp_path):
     for e in sc.surface_to_volume[sc.surface_elements]:
         assert tuple(sorted(e.tolist())) in tri_edges
     assert np.array_equal(sc.mesh_of_vertex, np.repeat([0, 1], 16))
+
+
+def test_deformable_solid_controls_raise_clearly():
+    p = F.SimulationParameters2D(fluid_nx=8, fluid_ny=8)
+    sim = F.Simulator2D(p)
+    for call in (lambda: sim.apply_lbs_control(0, [], []), lambda: sim.apply_active_strain(0, []),
+                 lambda: sim.getLBSVertices()):
+        try:
+            call()
+        except NotImplementedError:
+            pass
+        else:
+            raise AssertionError("expected NotImplementedError")
+    assert sim.getControlPointIdx() == []
