@@ -678,7 +678,9 @@ def run_ours(args):
     dense_ms, dense_n = prof["dense"]
     dense_avg_s = dense_ms * 1e-3 / max(1, dense_n)
     achieved = wl.ncell * bpc / dense_avg_s / 1e9
-    launches_per_step = 1 + (3 if surf is not None else 0)
+    # dense pass, plus detection, link cells and (for surfaces of more than
+    # 2048 force components) the force conversion
+    launches_per_step = 1 + ((3 if surf.num_vertices * wl.dim > 2048 else 2) if surf is not None else 0)
     tpc = DENSE_TRAFFIC_PER_CELL.get((wl.dim, storage))
     traffic = round(tpc[0] * wl.ncell) if tpc else None
     traffic_src = f"{tpc[0]} B/cell measured by ncu, scaled to {wl.ncell} cells ({tpc[1]})" if tpc else None

@@ -6,7 +6,8 @@
 //                                             concurrent with 2
 //   2. dense2d/dense3d                         O(grid), the bandwidth-bound pass
 //   3. link_cells     (only with a surface)   O(boundary cells), after 1 and 2
-//   4. finalize_forces(only with a surface)   O(vertices)
+//   4. finalize_forces(only with a surface)   O(vertices); folded into the
+//                                             last CTA of 3 for small surfaces
 // then the host flips the current buffer, exactly where the reference calls
 // flow_field.swapMoments() (FsiCoupling2D.cu:419, FsiCoupling3D.cu:476).
 #include <algorithm>
@@ -131,8 +132,10 @@ ffs_status ensure_links(ffs_lbm *h, int64_t max_vertices, int64_t max_link_cells
         lt.cap = want_cap;
     }
     if (!lt.count) {
-        FFS_CK(cudaMalloc(&lt.count, sizeof(uint32_t)));
-        FFS_CK(cudaMemset(lt.count, 0, sizeof(uint32_t)));
+        // the list count and the finished-CTA count of link_cells_kernel
+        FFS_CK(cudaMalloc(&lt.count, 2 * sizeof(uint32_t)));
+        FFS_CK(cudaMemset(lt.count, 0, 2 * sizeof(uint32_t)));
+        lt.done = lt.count + 1;
     }
     if ((int64_t)lt.acc_cap < max_vertices) {
         cudaFree(lt.acc);
@@ -241,12 +244,15 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const SurfaceArg
     }
     if (surf) {
         FFS_CK(cudaStreamWaitEvent(st, h->join, 0));
+        const bool fold = (long long)sa.nv * DIM <= kFoldForcesMax;
         {
             StageTimer t(h, 2, st);
-            FFS_CK((launch_link_cells<DIM, T>(g, words, h->lt, sa, sc, st)));
+            FFS_CK((launch_link_cells<DIM, T>(g, words, h->lt, sa, sc, st, fold)));
         }
-        StageTimer t(h, 3, st);
-        FFS_CK(launch_finalize_forces<DIM>(h->lt, sa, h->cf, st));
+        if (!fold) {
+            StageTimer t(h, 3, st);
+            FFS_CK(launch_finalize_forces<DIM>(h->lt, sa, h->cf, st));
+        }
     }
     h->cur ^= 1;
     return FFS_OK;
@@ -708,7 +714,7 @@ ffs_status ffs_lbm_profile_read(ffs_lbm *h, ffs_profile *out, int reset)
 // Scratch layout (one array shared by every grid and every call on a device):
 //   keys  [kNoallocSlots]  u32, 0 = empty slot          must start at 0
 //   list  [kNoallocSlots]  u32, claimed slots            no requirement
-//   count u32 (own 256-byte line)                        must start at 0
+//   count, done u32 (own 256-byte line)                  must start at 0
 //   links [kNoallocSlots * Q] u64, ~0 = no link          must start at ~0
 //   acc   [kNoallocMaxVertices * DIM] i64 force sums     must start at 0
 // Every call clears all four on its stream before its first kernel, so a
@@ -773,6 +779,7 @@ template <int DIM, typename T> ffs_status noalloc_impl(ffs_lbm *h, const ffs_sur
         lt.keys = reinterpret_cast<uint32_t *>(base + kNoallocKeysOff);
         lt.list = reinterpret_cast<uint32_t *>(base + kNoallocListOff);
         lt.count = reinterpret_cast<uint32_t *>(base + kNoallocCountOff);
+        lt.done = lt.count + 1; // same 256-byte line, cleared with it
         lt.links = reinterpret_cast<unsigned long long *>(base + kNoallocLinksOff);
         lt.acc = reinterpret_cast<long long *>(base + kNoallocAccOff);
         lt.acc_cap = kNoallocMaxVertices;
@@ -784,8 +791,9 @@ template <int DIM, typename T> ffs_status noalloc_impl(ffs_lbm *h, const ffs_sur
     if (DIM == 2) FFS_CK(launch_dense2d<T>(g, st));
     else FFS_CK(launch_dense3d<T>(g, st, h->dense_variant < 0 ? 0 : h->dense_variant));
     if (surf) {
-        FFS_CK((launch_link_cells<DIM, T>(g, words, lt, sa, sc, st)));
-        FFS_CK(launch_finalize_forces<DIM>(lt, sa, h->cf, st));
+        const bool fold = (long long)sa.nv * DIM <= kFoldForcesMax;
+        FFS_CK((launch_link_cells<DIM, T>(g, words, lt, sa, sc, st, fold)));
+        if (!fold) FFS_CK(launch_finalize_forces<DIM>(lt, sa, h->cf, st));
     }
     h->cur ^= 1;
     return FFS_OK;

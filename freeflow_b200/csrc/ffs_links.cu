@@ -158,9 +158,27 @@ __global__ void __launch_bounds__(256) detect_links2_kernel(GridArgs<T> g, uint3
 }
 
 // -------------------------------------------------------------- link cells
+// One fixed-point force sum -> physical force: added to the surface's force
+// arrays, or, in the coupled step, written to the mapped volume vertex (whose
+// force the gather zeroed), as scatterSurfaceForcesToVolume assigns it
+// (src/fsi/FsiCouplingKernels.cu:59-90).
+template <int DIM>
+__device__ __forceinline__ void finalize_force(const SurfaceArgs &s, long long t, long long a, double cf)
+{
+    double f = (double)a * (1.0 / kForceScale) * cf;
+    if (s.vforces) {
+        const long long i = t / DIM;
+        const uint32_t m = s.map[i];
+        if (m < (uint32_t)s.nvol) s.vforces[(size_t)m * DIM + (t - i * DIM)] = (float)f;
+    } else {
+        if (s.forces) s.forces[t] += (float)f;
+        if (s.forces64) s.forces64[t] += f;
+    }
+}
+
 template <int DIM, typename T, bool HALF>
 __global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
-                                                         StepScalars sc)
+                                                         StepScalars sc, bool fold_forces)
 {
     constexpr int Q = Lattice<DIM>::Q, G = kLinkGroup<DIM>, kPerWarp = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -181,6 +199,31 @@ __global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint3
             set_link_bit(flag_words, cell, false);
         }
     }
+    if (!fold_forces) return;
+    // The CTA that finishes last converts the force sums: every other CTA's
+    // atomics are complete and fenced before its count.  No CTA waits for
+    // another.  The counters are reset for the next step.
+    __shared__ bool last_cta;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last_cta = atomicAdd(lt.done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last_cta) return;
+    __threadfence();
+    const long long nf = (long long)s.nv * DIM;
+    for (long long t = threadIdx.x; t < nf; t += blockDim.x) {
+        const long long a = __ldcg(lt.acc + t);
+        if (a != 0) {
+            finalize_force<DIM>(s, t, a, sc.cf);
+            lt.acc[t] = 0;
+        }
+    }
+    if (threadIdx.x == 0) {
+        *lt.count = 0;
+        *lt.done = 0;
+    }
 }
 
 // Fixed-point sums -> physical forces: added to the surface's force arrays,
@@ -194,15 +237,7 @@ __global__ void finalize_forces_kernel(LinkTable lt, SurfaceArgs s, double cf)
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         long long a = lt.acc[t];
         if (a != 0) {
-            double f = (double)a * (1.0 / kForceScale) * cf;
-            if (s.vforces) {
-                const long long i = t / DIM;
-                const uint32_t m = s.map[i];
-                if (m < (uint32_t)s.nvol) s.vforces[(size_t)m * DIM + (t - i * DIM)] = (float)f;
-            } else {
-                if (s.forces) s.forces[t] += (float)f;
-                if (s.forces64) s.forces64[t] += f;
-            }
+            finalize_force<DIM>(s, t, a, cf);
             lt.acc[t] = 0;
         }
     }
@@ -273,17 +308,17 @@ cudaError_t launch_detect_links(const GridArgs<T> &g, uint32_t *flag_words, cons
 
 template <int DIM, typename T>
 cudaError_t launch_link_cells(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
-                              const StepScalars &sc, cudaStream_t st)
+                              const StepScalars &sc, cudaStream_t st, bool fold_forces)
 {
     // persistent warps over the device-side count, one wave: as many CTAs of
     // 8 warps as are resident together (a CTA beyond that would run its fixed
     // share of the cells after the others finish)
     if (g.half_pops)
         link_cells_kernel<DIM, T, true><<<resident_grid<link_cells_kernel<DIM, T, true>>(256), 256, 0, st>>>(
-            g, flag_words, lt, s, sc);
+            g, flag_words, lt, s, sc, fold_forces);
     else
         link_cells_kernel<DIM, T, false><<<resident_grid<link_cells_kernel<DIM, T, false>>(256), 256, 0, st>>>(
-            g, flag_words, lt, s, sc);
+            g, flag_words, lt, s, sc, fold_forces);
     return cudaGetLastError();
 }
 
@@ -320,7 +355,7 @@ cudaError_t launch_reset_links(const LinkTable &lt, uint32_t *flag_words, cudaSt
     template cudaError_t launch_detect_links<DIM, T>(const GridArgs<T> &, uint32_t *, const LinkTable &,              \
                                                      const SurfaceArgs &, const StepScalars &, cudaStream_t);          \
     template cudaError_t launch_link_cells<DIM, T>(const GridArgs<T> &, uint32_t *, const LinkTable &,                \
-                                                   const SurfaceArgs &, const StepScalars &, cudaStream_t);
+                                                   const SurfaceArgs &, const StepScalars &, cudaStream_t, bool);
 FFS_INST_LINKS(2, float)
 FFS_INST_LINKS(2, __half)
 FFS_INST_LINKS(2, __nv_bfloat16)

@@ -19,7 +19,14 @@ struct LinkTable {
     uint32_t *count = nullptr;         // [1]
     long long *acc = nullptr;          // [acc_cap * DIM] fixed-point force sums (2^-32 units)
     uint32_t acc_cap = 0;              // vertices
+    uint32_t *done = nullptr;          // [1] CTAs of link_cells_kernel that finished (zero between steps)
 };
+
+// Surfaces of at most this many force components have their fixed-point
+// sums converted by the last CTA of link_cells_kernel instead of a kernel of
+// their own: one launch less per step where launches dominate (the 2D
+// configurations), one CTA's work where that is cheap.
+constexpr long long kFoldForcesMax = 2048;
 
 struct SurfaceArgs {
     const float *V;
@@ -47,9 +54,11 @@ constexpr double kForceScale = 4294967296.0; // 2^32
 template <int DIM, typename T>
 cudaError_t launch_detect_links(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
                                 const StepScalars &sc, cudaStream_t st);
+// With fold_forces, the last CTA also does launch_finalize_forces's work
+// (the caller launches no finalize kernel); lt.done must be allocated.
 template <int DIM, typename T>
 cudaError_t launch_link_cells(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
-                              const StepScalars &sc, cudaStream_t st);
+                              const StepScalars &sc, cudaStream_t st, bool fold_forces = false);
 template <int DIM>
 cudaError_t launch_finalize_forces(const LinkTable &lt, const SurfaceArgs &s, double cf, cudaStream_t st);
 template <int DIM>

@@ -237,7 +237,9 @@ ffs_status ffs_lbm_debug_links(ffs_lbm *grid, const ffs_surface *surface, uint64
  * enabled, each step records CUDA events around its stages on the step's
  * stream; ffs_lbm_profile_read() waits for the recorded events and returns
  * the summed milliseconds and launch counts per stage:
- * [0] link detection, [1] dense fused update, [2] link cells, [3] forces. */
+ * [0] link detection, [1] dense fused update, [2] link cells, [3] forces.
+ * For surfaces of at most 2048 force components the force conversion runs in
+ * the last CTA of the link-cell kernel, and [3] records no launch. */
 typedef struct {
     double ms[4];
     int64_t launches[4];
