@@ -176,9 +176,9 @@ __device__ __forceinline__ void finalize_force(const SurfaceArgs &s, long long t
     }
 }
 
-template <int DIM, typename T, bool HALF>
+template <int DIM, typename T, bool HALF, bool FOLD>
 __global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt, SurfaceArgs s,
-                                                         StepScalars sc, bool fold_forces)
+                                                         StepScalars sc)
 {
     constexpr int Q = Lattice<DIM>::Q, G = kLinkGroup<DIM>, kPerWarp = 32 / G;
     const int lane = threadIdx.x & (G - 1);
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(256, 5) link_cells_kernel(GridArgs<T> g, uint3
             set_link_bit(flag_words, cell, false);
         }
     }
-    if (!fold_forces) return;
+    if constexpr (!FOLD) return;
     // The CTA that finishes last converts the force sums: every other CTA's
     // atomics are complete and fenced before its count.  No CTA waits for
     // another.  The counters are reset for the next step.
@@ -306,6 +306,14 @@ cudaError_t launch_detect_links(const GridArgs<T> &g, uint32_t *flag_words, cons
     return cudaGetLastError();
 }
 
+template <int DIM, typename T, bool HALF, bool FOLD>
+static void launch_link_cells_as(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
+                                 const StepScalars &sc, cudaStream_t st)
+{
+    link_cells_kernel<DIM, T, HALF, FOLD>
+        <<<resident_grid<link_cells_kernel<DIM, T, HALF, FOLD>>(256), 256, 0, st>>>(g, flag_words, lt, s, sc);
+}
+
 template <int DIM, typename T>
 cudaError_t launch_link_cells(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt, const SurfaceArgs &s,
                               const StepScalars &sc, cudaStream_t st, bool fold_forces)
@@ -313,12 +321,13 @@ cudaError_t launch_link_cells(const GridArgs<T> &g, uint32_t *flag_words, const 
     // persistent warps over the device-side count, one wave: as many CTAs of
     // 8 warps as are resident together (a CTA beyond that would run its fixed
     // share of the cells after the others finish)
-    if (g.half_pops)
-        link_cells_kernel<DIM, T, true><<<resident_grid<link_cells_kernel<DIM, T, true>>(256), 256, 0, st>>>(
-            g, flag_words, lt, s, sc, fold_forces);
-    else
-        link_cells_kernel<DIM, T, false><<<resident_grid<link_cells_kernel<DIM, T, false>>(256), 256, 0, st>>>(
-            g, flag_words, lt, s, sc, fold_forces);
+    if (g.half_pops) {
+        if (fold_forces) launch_link_cells_as<DIM, T, true, true>(g, flag_words, lt, s, sc, st);
+        else launch_link_cells_as<DIM, T, true, false>(g, flag_words, lt, s, sc, st);
+    } else {
+        if (fold_forces) launch_link_cells_as<DIM, T, false, true>(g, flag_words, lt, s, sc, st);
+        else launch_link_cells_as<DIM, T, false, false>(g, flag_words, lt, s, sc, st);
+    }
     return cudaGetLastError();
 }
 
