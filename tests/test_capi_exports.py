@@ -79,3 +79,48 @@ def test_pool_descriptor_checks_need_no_device():
     assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
     d.num_actions, d.budget_bytes = 8, 0
     assert L.ffs_pool_create(ctypes.byref(d), ctypes.byref(h)) == 1
+
+
+def test_step_entry_points_reject_null_arguments_without_device_work():
+    L = _capi.load()
+    vs = _capi.VolumeSurface()
+    s = _capi.Surface()
+    assert L.ffs_lbm_step_coupled(None, ctypes.byref(vs), None) == 1
+    assert b"null" in L.ffs_last_error()
+    assert L.ffs_lbm_step(None, ctypes.byref(s), None) == 1
+    assert L.ffs_lbm_step_noalloc(None, ctypes.byref(s), None) == 1
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the C layout: a C program built
+    against include/ffs_lbm.h and include/ffs_pool.h prints sizeof and every
+    field's offsetof."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    structs = {"ffs_surface": _capi.Surface, "ffs_volume_surface": _capi.VolumeSurface, "ffs_lbm_desc": _capi.LbmDesc,
+               "ffs_profile": _capi.Profile, "ffs_pool_desc": _capi.PoolDesc, "ffs_swimmer": _capi.Swimmer,
+               "ffs_episode_desc": _capi.EpisodeDesc, "ffs_pool_output": _capi.PoolOutput,
+               "ffs_pool_info": _capi.PoolInfo}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "ffs_lbm.h"', '#include "ffs_pool.h"',
+             "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = str(tmp_path / "layout")
+    r = subprocess.run(["gcc", "-std=c11", "-I" + os.path.join(ROOT, "include"), str(src), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split() for line in subprocess.run([exe], capture_output=True, text=True).stdout.splitlines())
+    for cname, cls in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, f"{cname}.{fname}"
