@@ -102,17 +102,17 @@ class VolumeSurface:
     def __init__(self, volume_positions, volume_velocities, surface_to_volume, elements, device="cuda"):
         import torch
 
+        # torch.tensor copies: the object never aliases the caller's arrays
         vp = np.ascontiguousarray(volume_positions, dtype=np.float32)
         self.dim = int(vp.shape[1])
-        self.volume_positions = torch.as_tensor(vp, device=device).contiguous()
-        self.volume_velocities = torch.as_tensor(np.ascontiguousarray(volume_velocities, dtype=np.float32),
-                                                 device=device).contiguous()
+        self.volume_positions = torch.tensor(vp, device=device)
+        self.volume_velocities = torch.tensor(np.ascontiguousarray(volume_velocities, dtype=np.float32), device=device)
         assert self.volume_velocities.shape == self.volume_positions.shape
         self.volume_forces = torch.zeros_like(self.volume_positions)
         m = np.ascontiguousarray(surface_to_volume, dtype=np.uint32).reshape(-1)
-        self.surface_to_volume = torch.as_tensor(m.view(np.int32), device=device).contiguous()
+        self.surface_to_volume = torch.tensor(m.view(np.int32), device=device)
         e = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1, self.dim)
-        self.elements = torch.as_tensor(e.view(np.int32), device=device).contiguous()
+        self.elements = torch.tensor(e.view(np.int32), device=device)
         self.surface_positions = torch.zeros((m.size, self.dim), dtype=torch.float32, device=device)
         self.surface_velocities = torch.zeros_like(self.surface_positions)
 

@@ -124,3 +124,30 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
         assert int(got[cname]) == ctypes.sizeof(cls), cname
         for fname, _ in cls._fields_:
             assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, f"{cname}.{fname}"
+
+
+def test_volume_surface_struct_plumbing_on_the_host():
+    """VolumeSurface fills every ffs_volume_surface field from its tensors (built on
+    the CPU here; no library call is made)."""
+    import numpy as np
+
+    from freeflow_b200 import VolumeSurface
+
+    rng = np.random.default_rng(0)
+    vp = rng.standard_normal((10, 3)).astype(np.float32)
+    vv = rng.standard_normal((10, 3)).astype(np.float32)
+    smap = np.array([7, 2, 5, 0], np.uint32)
+    elems = np.array([[0, 1, 2], [1, 2, 3]], np.uint32)
+    vs = VolumeSurface(vp, vv, smap, elems, device="cpu")
+    s = vs.c_struct()
+    assert (s.dim, s.num_volume_vertices, s.num_vertices, s.num_elements) == (3, 10, 4, 2)
+    for name in ("volume_positions", "volume_velocities", "volume_forces", "surface_to_volume", "elements",
+                 "surface_positions", "surface_velocities"):
+        assert getattr(s, name), name
+    assert s.volume_positions == vs.volume_positions.data_ptr()
+    assert np.array_equal(vs.surface_to_volume.numpy().view(np.uint32), smap)
+    assert vs.surface_positions.shape == (4, 3) and vs.volume_forces.shape == (10, 3)
+    moved = vp + 1.0
+    vs.update(moved, None)
+    assert np.array_equal(vs.volume_positions.numpy(), moved) and np.array_equal(vs.volume_velocities.numpy(), vv)
+    assert not np.array_equal(vp, moved)          # the caller's array is not aliased
