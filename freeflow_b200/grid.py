@@ -42,13 +42,13 @@ class DeviceSurface:
     def __init__(self, vertices, velocities, elements, device="cuda", with_forces64=False):
         import torch
 
-        v = torch.as_tensor(np.ascontiguousarray(vertices, dtype=np.float32), device=device)
-        self.dim = int(v.shape[1])
-        self.vertices = v.contiguous()
-        self.velocities = torch.as_tensor(np.ascontiguousarray(velocities, dtype=np.float32), device=device).contiguous()
+        # torch.tensor copies: the object never aliases the caller's arrays
+        self.vertices = torch.tensor(np.ascontiguousarray(vertices, dtype=np.float32), device=device)
+        self.dim = int(self.vertices.shape[1])
+        self.velocities = torch.tensor(np.ascontiguousarray(velocities, dtype=np.float32), device=device)
         e = np.ascontiguousarray(elements, dtype=np.uint32).reshape(-1, self.dim)
         # torch has no uint32 arithmetic we need; keep raw bytes in int32
-        self.elements = torch.as_tensor(e.view(np.int32), device=device).contiguous()
+        self.elements = torch.tensor(e.view(np.int32), device=device)
         self.forces = torch.zeros_like(self.vertices)
         self.forces64 = torch.zeros(self.vertices.shape, dtype=torch.float64, device=device) if with_forces64 else None
         assert self.velocities.shape == self.vertices.shape
