@@ -36,7 +36,10 @@
 #include "ffs_f2.cuh"
 
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <utility>
 
 namespace fflbm {
 
@@ -406,6 +409,33 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     if (p <= ze) plane(p, X, Y);
 }
 
+// CTAs of `kernel` resident on the current device at once (SMs x occupancy),
+// with the kernel's dynamic shared-memory limit raised to `smem` first.
+// Cached per (kernel, device ordinal): a process may step grids on several
+// GPUs, and the first launch on each device configures the kernel there.
+static cudaError_t resident_slots(const void *kernel, int threads, size_t smem, int &slots)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({kernel, dev});
+    if (it != cache.end()) {
+        slots = it->second;
+        return cudaSuccess;
+    }
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (e != cudaSuccess) return e;
+    slots = device_sms() * (per_sm > 0 ? per_sm : 1);
+    cache[{kernel, dev}] = slots;
+    return cudaSuccess;
+}
+
 // Number of z chunks that best fills the GPU: whole waves of CTAs, with the
 // two extra planes each chunk reconstructs counted as overhead.
 static int choose_zchunks(int tiles, int nz, int slots)
@@ -430,18 +460,10 @@ static int choose_zchunks(int tiles, int nz, int slots)
 template <typename T, int MINB, bool IDX32> struct Dense3dLaunchAs {
     static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
     {
-        static bool configured = false;
-        static int slots = 0;
-        if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(dense3d_kernel<T, MINB, IDX32>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D3::kSmemBytes);
-            if (e != cudaSuccess) return e;
-            int per_sm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense3d_kernel<T, MINB, IDX32>, D3::kThreads,
-                                                          D3::kSmemBytes);
-            slots = device_sms() * (per_sm > 0 ? per_sm : 1);
-            configured = true;
-        }
+        int slots = 0;
+        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_kernel<T, MINB, IDX32>), D3::kThreads,
+                                       D3::kSmemBytes, slots);
+        if (e != cudaSuccess) return e;
         int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY;
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
@@ -740,20 +762,10 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_pair_kernel(GridAr
 template <int MINB> struct Dense3dPairLaunch {
     static cudaError_t run(const GridArgs<float> &g, cudaStream_t s)
     {
-        static bool configured = false;
-        static int slots = 0;
-        if (!configured) {
-            cudaError_t e = cudaFuncSetAttribute(dense3d_pair_kernel<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)kPairSmemBytes);
-            if (e != cudaSuccess) return e;
-            int dev = 0, sms = 0, per_sm = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense3d_pair_kernel<MINB>, D3::kThreads,
-                                                          kPairSmemBytes);
-            slots = sms * (per_sm > 0 ? per_sm : 1);
-            configured = true;
-        }
+        int slots = 0;
+        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_pair_kernel<MINB>), D3::kThreads,
+                                       kPairSmemBytes, slots);
+        if (e != cudaSuccess) return e;
         int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY;
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
