@@ -11,8 +11,11 @@ fraction of the measured HBM peak.
                   [--workload D|C|B|A] [--storage f32|f16|bf16] [--small]
 
 N > 1 runs one independent replica per GPU (one grid per GPU: the grid is not
-sharded, so there is no exchange step), launched by torchrun; the time is the
-max over ranks and value = all cells updated / that time ("weak").
+sharded, so there is no exchange step), one process per GPU: started by
+torchrun, or by bench.py itself when no launcher set WORLD_SIZE; the time is
+the max over ranks and value = all cells updated / that time ("weak").
+``--check-ranks`` only joins the ranks over gloo (no GPU work) and prints
+what every rank saw, a check of the launch.
 
 ``--impl reference`` times the reference's algorithm on the host cores: the
 FP32 restatement in oracle/ (the reference's CUDA sources do not build here)
@@ -67,6 +70,20 @@ def algorithmic_bytes_per_cell(dim: int, storage: str) -> int:
     nm = 6 if dim == 2 else 10
     s = 4 if storage == "f32" else 2
     return 2 * nm * s + 1
+
+
+def run_config(wl, storage: str, world: int) -> dict:
+    """The `config` object of both arms' JSON lines (the same dict, so the two
+    lines name the same workload)."""
+    bpc = algorithmic_bytes_per_cell(wl.dim, storage)
+    small = wl.ncell * bpc <= 2 * 126e6   # one moment buffer can sit in the 126 MB L2
+    surface = None
+    if wl.elements is not None:
+        surface = f"{wl.rest.shape[0]} vertices / {wl.elements.shape[0]} elements"
+    return {"workload": wl.name, "cells": wl.ncell, "storage": storage, "surface": surface,
+            "l2": ("moment buffers exceed L2 (no flush needed)" if not small
+                   else "L2 flushed before every step (256 MB write outside the timed spans)"),
+            "parallelism": f"replicas x{world}"}
 
 
 def make_workload(name: str, small: bool):
@@ -340,7 +357,7 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": round(1e3 * sec / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "impl": "reference",
-        "config": {"workload": wl.name, "cells": wl.ncell, "storage": "f32"},
+        "config": run_config(wl, "f32", args.gpus),
         "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -693,12 +710,8 @@ def run_ours(args):
             "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
             "warmup": Wm, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": storage, "data": "synthetic (seeded)",
-            "config": {"workload": wl.name, "cells": wl.ncell, "storage": storage,
-                       "surface": (f"{surf.num_vertices} vertices / {surf.num_elements} elements" if surf else None),
-                       "links_at_step0": link_stats,
-                       "l2": ("moment buffers exceed L2 (no flush needed)" if not small
-                              else "L2 flushed before every step (256 MB write outside the timed spans)"),
-                       "parallelism": f"replicas x{world}"},
+            "config": run_config(wl, storage, world),
+            "links_at_step0": link_stats,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
                          "peak_kind": peak_kind,
@@ -724,6 +737,19 @@ def run_ours(args):
     return 0
 
 
+def check_ranks():
+    """`--check-ranks`: join the ranks over gloo and print what each one saw."""
+    from freeflow_b200 import replicas as R
+
+    rank, world, local = R.env_ranks()
+    R.init("gloo", timeout_s=60.0)
+    seen = R.all_gather_objects({"rank": rank, "world": world, "local_rank": local, "pid": os.getpid()})
+    if rank == 0:
+        print(json.dumps({"check_ranks": seen}), flush=True)
+    R.shutdown()
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -735,7 +761,15 @@ def main():
     p.add_argument("--small", action="store_true", help="reduced grid (profiling captures)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the serving (config E) sub-measurement")
+    p.add_argument("--check-ranks", action="store_true", help="only join the ranks (gloo) and report them")
     args = p.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # no launcher: start one process per GPU here, as torchrun would
+        from freeflow_b200 import replicas as R
+
+        return R.launch_local_ranks([os.path.abspath(__file__), *sys.argv[1:]], args.gpus)
+    if args.check_ranks:
+        return check_ranks()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

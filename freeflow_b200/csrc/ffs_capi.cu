@@ -711,7 +711,9 @@ ffs_status ffs_lbm_profile_read(ffs_lbm *h, ffs_profile *out, int reset)
 // ffs_lbm_step allocates its scratch on the first step with a surface (and
 // again for a larger one); this entry point never does.
 //
-// Scratch layout (one array shared by every grid and every call on a device):
+// Scratch layout (one array shared by every grid and every call on a device;
+// the table has twice as many slots as the supported link cells, so it is at
+// most half full, like the table ffs_lbm_step sizes for itself):
 //   keys  [kNoallocSlots]  u32, 0 = empty slot          must start at 0
 //   list  [kNoallocSlots]  u32, claimed slots            no requirement
 //   count, done u32 (own 256-byte line)                  must start at 0
@@ -723,16 +725,20 @@ ffs_status ffs_lbm_profile_read(ffs_lbm *h, ffs_profile *out, int reset)
 // race on the array: the caller orders them.
 namespace {
 
-constexpr uint32_t kNoallocSlots = 16384;       // link cells per step at most
-constexpr uint32_t kNoallocMaxVertices = 32768; // surface vertices at most
+constexpr uint32_t kNoallocMaxLinkCells = 16384;          // link cells per step supported
+constexpr uint32_t kNoallocSlots = 2 * kNoallocMaxLinkCells; // table slots (full at 32,768 link cells)
+constexpr uint32_t kNoallocMaxVertices = 32768;           // surface vertices at most
 constexpr size_t kNoallocKeysOff = 0;
 constexpr size_t kNoallocListOff = kNoallocKeysOff + sizeof(uint32_t) * kNoallocSlots;
 constexpr size_t kNoallocCountOff = kNoallocListOff + sizeof(uint32_t) * kNoallocSlots;
 constexpr size_t kNoallocLinksOff = kNoallocCountOff + 256;
 constexpr size_t kNoallocAccOff = kNoallocLinksOff + sizeof(unsigned long long) * kNoallocSlots * 27;
-constexpr size_t kNoallocBytes = kNoallocAccOff + sizeof(long long) * kNoallocMaxVertices * 3; // 4,456,704
+constexpr size_t kNoallocBytes = kNoallocAccOff + sizeof(long long) * kNoallocMaxVertices * 3; // 8,126,720
 static_assert(kNoallocLinksOff % 256 == 0 && kNoallocAccOff % 256 == 0, "scratch sections stay 256-byte aligned");
 static_assert((kNoallocSlots & (kNoallocSlots - 1)) == 0, "the link table wants a power-of-two slot count");
+static_assert(kNoallocBytes == 8126720, "the header states the scratch size");
+static_assert(kNoallocMaxLinkCells == FFS_NOALLOC_MAX_LINK_CELLS && kNoallocMaxVertices == FFS_NOALLOC_MAX_VERTICES,
+              "limits as the header states them");
 
 constexpr int kNoallocMaxDevices = 64;
 
@@ -747,6 +753,8 @@ unsigned char *g_noalloc_base[kNoallocMaxDevices] = {};
 
 // Address of the scratch array on the current device, looked up once per
 // device (the lookup may load this library's device code on that device).
+// A cudaDeviceReset discards that code and with it the array, so the cached
+// address is only valid until the device is reset (the header says so).
 ffs_status noalloc_scratch(unsigned char **out)
 {
     int dev = -1;
@@ -786,11 +794,17 @@ template <int DIM, typename T> ffs_status noalloc_impl(ffs_lbm *h, const ffs_sur
         FFS_CK(cudaMemsetAsync(base, 0, kNoallocLinksOff, st)); // keys, list, count
         FFS_CK(cudaMemsetAsync(lt.links, 0xFF, sizeof(unsigned long long) * kNoallocSlots * Q, st));
         FFS_CK(cudaMemsetAsync(lt.acc, 0, sizeof(long long) * (size_t)s->num_vertices * DIM, st));
-        FFS_CK((launch_detect_links<DIM, T>(g, words, lt, sa, sc, st)));
+        // detection on the grid's side stream, beside the dense pass, as in
+        // step_impl (the streams and events exist since the grid was created)
+        FFS_CK(cudaEventRecord(h->fork, st));
+        FFS_CK(cudaStreamWaitEvent(h->side, h->fork, 0));
+        FFS_CK((launch_detect_links<DIM, T>(g, words, lt, sa, sc, h->side)));
+        FFS_CK(cudaEventRecord(h->join, h->side));
     }
     if (DIM == 2) FFS_CK(launch_dense2d<T>(g, st));
     else FFS_CK(launch_dense3d<T>(g, st, h->dense_variant < 0 ? 0 : h->dense_variant));
     if (surf) {
+        FFS_CK(cudaStreamWaitEvent(st, h->join, 0));
         const bool fold = (long long)sa.nv * DIM <= kFoldForcesMax;
         FFS_CK((launch_link_cells<DIM, T>(g, words, lt, sa, sc, st, fold)));
         if (!fold) FFS_CK(launch_finalize_forces<DIM>(lt, sa, h->cf, st));

@@ -187,18 +187,24 @@ ffs_status ffs_lbm_step_coupled(ffs_lbm *grid, const ffs_volume_surface *surface
 
 /* No counterpart in the reference.  The same step as ffs_lbm_step, with the
  * same results, but it allocates no device memory: its link table and force
- * accumulators live in one fixed array inside this library (4,456,704 bytes
+ * accumulators live in one fixed array inside this library (8,126,720 bytes
  * per device), for callers that must not allocate while stepping (a fixed,
  * pre-reserved device-memory budget; loops that cannot afford the device-wide
  * synchronisation of cudaMalloc/cudaFree).
  * Limits: at most FFS_NOALLOC_MAX_VERTICES surface vertices (larger surfaces
- * return FFS_ERR_CAPACITY before any work); at most FFS_NOALLOC_MAX_LINK_CELLS
- * cells may own links in one step (more latch status bit 2, link table
- * overflow, like ffs_lbm_step with a too-small reservation).
+ * return FFS_ERR_CAPACITY before any work).  FFS_NOALLOC_MAX_LINK_CELLS cells
+ * may own links in one step with the table at most half full; past that the
+ * step still runs but detection slows as the table fills, and at twice that
+ * number the table is full and the step latches status bit 2 (link table
+ * overflow, as ffs_lbm_step does with a too-small reservation).
  * The first call on a device looks the array up on that device (set-up): make
- * it before any stream capture.  Every call on a device shares the array and
- * clears it on `stream` first, so calls that overlap in time on one device
- * race: the caller orders them (one stream, or events). */
+ * it before any stream capture.  The address is kept for the process; after
+ * a cudaDeviceReset of that device this entry point must not be called again.
+ * Every call on a device shares the array and clears it on `stream` first, so
+ * calls that overlap in time on one device race: the caller orders them (one
+ * stream, or events).  Link detection runs beside the dense pass on the
+ * grid's side stream, as in ffs_lbm_step; stage timing
+ * (ffs_lbm_profile_enable) records nothing for these steps. */
 #define FFS_NOALLOC_MAX_VERTICES 32768
 #define FFS_NOALLOC_MAX_LINK_CELLS 16384
 ffs_status ffs_lbm_step_noalloc(ffs_lbm *grid, const ffs_surface *surface, void *stream);

@@ -1,6 +1,8 @@
 """The multi-rank protocol of bench.py (one replica per GPU, max-over-ranks
-timing, whole-job rate), run as two gloo ranks on the CPU; and the rank != 0
-exit of the CPU reference arm."""
+timing, whole-job rate), run as two gloo ranks on the CPU; the rank != 0
+exit of the CPU reference arm; and bench.py starting its own ranks when no
+launcher set WORLD_SIZE."""
+import json
 import os
 import socket
 import subprocess
@@ -68,3 +70,26 @@ def test_reference_arm_exits_on_other_ranks():
                        env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_bench_starts_its_own_ranks():
+    """`bench.py --gpus 2` without a launcher runs two processes, ranks 0 and 1
+    of a world of 2, which meet over gloo (--check-ranks does no GPU work)."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--check-ranks"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1                        # rank 0 prints, rank 1 does not
+    seen = json.loads(lines[0])["check_ranks"]
+    assert [(x["rank"], x["world"], x["local_rank"]) for x in seen] == [(0, 2, 0), (1, 2, 1)]
+    assert seen[0]["pid"] != seen[1]["pid"]       # two processes
+
+
+def test_bench_launch_reports_a_failed_rank():
+    """A rank that fails makes the launch fail (its exit code comes back)."""
+    sys.path.insert(0, ROOT)
+    from freeflow_b200 import replicas as R
+
+    code = "import os, sys; sys.exit(3 if os.environ['RANK'] == '1' else 0)"
+    assert R.launch_local_ranks(["-c", code], 2) == 3
