@@ -313,16 +313,29 @@ def tgv_velocity_errors(storages=("f32", "f16", "bf16"), n: int = 48, steps: int
 
 def cpu_leg(wl: W.Workload, threads: int):
     """The CPU leg of the GPU arm, the one place where this arm runs the oracle:
-    the oracle's FP32 restatement timed on the host cores (the CPU baseline, a
-    z-slab sample of about 20 s of CPU work), and the oracle's FP64 build as
-    the checker of the reduced-storage GPU outputs.  Returns (cpu_baseline,
-    errors against FP64)."""
-    rate = 4.0e6 * threads / 8.0
-    nz_slab = int(20.0 * rate / 3 / (wl.nx * wl.ny)) if wl.dim == 3 else 1
-    mlups, cells, sec = oracle_slab_run(wl, 3, 1, nz_slab, threads)
-    cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-           "sample": (f"3 steps of a {cells // (wl.nx * wl.ny)}-plane z-slab of {wl.name}" if wl.dim == 3
-                      else f"3 steps of {wl.name}") + f", FP32 restatement, {sec:.1f} s"}
+    the oracle's FP64 build timed on the host cores at all threads and at one
+    (the CPU baseline: an FP64 run of the same update), its FP32 restatement
+    beside it, each on a z-slab sample of the workload sized to about 10-20 s
+    of CPU work; and the FP64 build as the checker of the reduced-storage GPU
+    outputs.  Returns (cpu_baseline, errors against FP64)."""
+    def slab(seconds, rate):
+        return int(seconds * rate / 3 / (wl.nx * wl.ny)) if wl.dim == 3 else 1
+
+    rate_all = 2.0e6 * threads          # cell updates / s of the oracle, measured order
+    mlups64, cells64, sec64 = oracle_slab_run(wl, 3, 1, slab(15.0, rate_all), threads, precision="phys64")
+    mlups32, cells32, sec32 = oracle_slab_run(wl, 3, 1, slab(15.0, rate_all), threads, precision="ref32")
+    mlups1, cells1, sec1 = oracle_slab_run(wl, 3, 1, slab(10.0, 2.0e6), 1, precision="phys64")
+    nxy = wl.nx * wl.ny
+
+    def sample(cells, sec, what):
+        return ((f"3 steps of a {cells // nxy}-plane z-slab of {wl.name}" if wl.dim == 3 else f"3 steps of {wl.name}")
+                + f", {what}, {sec:.1f} s")
+
+    cpu = {"value": round(mlups64, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+           "sample": sample(cells64, sec64, "FP64 oracle"),
+           "fp64_1_thread": {"value": round(mlups1, 3), "cores": 1, "sample": sample(cells1, sec1, "FP64 oracle")},
+           "fp32_all_threads": {"value": round(mlups32, 3), "cores": threads,
+                                "sample": sample(cells32, sec32, "FP32 restatement of the reference's arithmetic")}}
     errors = {
         "serving_2d": {
             "closed_tank": {"f16": serving_velocity_error("f16"), "f32": serving_velocity_error("f32")},
@@ -330,8 +343,9 @@ def cpu_leg(wl: W.Workload, threads: int):
                         "f32": serving_velocity_error("f32", sides="outlets")},
             "case": "pool episode, 256x128 swimmer, 200 substeps, same surfaces as the FP64 oracle; with outlets "
                     "the reference's sign-switched outlet rule makes even FP32 differ from FP64 (branch flips)"},
-        "taylor_green_3d": tgv_velocity_errors(),
-        "taylor_green_3d_case": "D3Q27 periodic 48^3, u0 0.04, viscosity 0.005, 100 steps, relative L2 of u",
+        "taylor_green_3d": tgv_velocity_errors(n=128, steps=200),
+        "taylor_green_3d_case": "config C itself: D3Q27 periodic 128^3, u0 0.04, viscosity 0.005, 200 steps, "
+                                "relative L2 of u against the FP64 oracle",
         "target": "f16 relative velocity error <= 1e-3",
     }
     return cpu, errors
@@ -368,46 +382,52 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- serving
-def run_serving(iterations: int, warmup: int, concurrency: int = 256, plain_steps: int = 20, seed: int = 0):
+def run_serving(iterations: int, warmup: int, concurrencies=(64, 256, 512), plain_steps: int = 20,
+                plain_seconds: float = 1.0, seed: int = 0):
     """Config E: Poisson stream of 2D swimmer episodes (grids uniform over
     256x128, 512x192, 1200x400; 8 actions per control step; 10 substeps per
     action; lengths uniform in 200..2000 control steps) through the FP16 pool
-    with continuous batching, against the plain per-episode FP32 path."""
+    with continuous batching, at each mean concurrency, against the plain
+    per-episode FP32 path (one episode of each grid size at a time, at least
+    `plain_seconds` of control steps each)."""
     import torch
     from freeflow_b200 import serving as S
 
-    mean_len = 1100.0
-    per_iter = concurrency / mean_len
-    n_specs = concurrency + int(per_iter * (iterations + warmup) * 1.5) + 16
-    specs = S.serving_mix(n_specs, seed=seed)
-    pool = S.Pool(storage="f16", budget_bytes=6 << 30, max_episodes=2 * concurrency, substeps=10, num_actions=8)
     t0 = time.perf_counter()
-    r = S.serve(pool, specs, iterations=iterations, initial=concurrency, arrivals_per_iter=per_iter, seed=seed,
-                warmup_iterations=warmup)
-    info = r.pop("pool_info_at_end")
-    pool.close()
-    torch.cuda.synchronize()
-    # plain path: one episode of each grid size, one at a time
-    sample = [S.make_episode(nx, ny, seed=1000 + i, length=plain_steps) for i, (nx, ny) in enumerate(S.SERVING_SIZES)]
-    plain = S.plain_rate(sample, plain_steps)
     peak, peak_kind = hbm_peak()
-    dense_gbs = info["tuned_cells"] * 25 / (info["dense_ms"] * 1e-3) / 1e9 if info["dense_ms"] > 0 else None
-    out = {
+    sample = [S.make_episode(nx, ny, seed=1000 + i, length=plain_steps) for i, (nx, ny) in enumerate(S.SERVING_SIZES)]
+    plain = S.plain_rate(sample, plain_steps, min_seconds=plain_seconds)
+    by_c = {}
+    for concurrency in concurrencies:
+        mean_len = 1100.0
+        per_iter = concurrency / mean_len
+        n_specs = concurrency + int(per_iter * (iterations + warmup) * 1.5) + 16
+        specs = S.serving_mix(n_specs, seed=seed)
+        max_episodes = min(1000, 2 * concurrency)   # the pool holds at most 1000 episodes
+        pool = S.Pool(storage="f16", budget_bytes=6 << 30, max_episodes=max_episodes, substeps=10, num_actions=8)
+        r = S.serve(pool, specs, iterations=iterations, initial=concurrency, arrivals_per_iter=per_iter, seed=seed,
+                    warmup_iterations=warmup)
+        info = r.pop("pool_info_at_end")
+        pool.close()
+        torch.cuda.synchronize()
+        dense_gbs = info["tuned_cells"] * 25 / (info["dense_ms"] * 1e-3) / 1e9 if info["dense_ms"] > 0 else None
+        by_c[str(concurrency)] = {
+            "batched": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()},
+            "speedup_vs_plain": round(r["env_steps_per_s"] / plain["env_steps_per_s"], 2),
+            "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}" + (" strip" if info["strip"] else ""),
+                     "graph_builds": info["graph_builds"], "max_episodes": max_episodes,
+                     "dense_ms_at_tuning": round(info["dense_ms"], 4), "cells_at_tuning": info["tuned_cells"],
+                     "dense_roofline": ({"achieved": round(dense_gbs, 1), "peak": peak, "unit": "GB/s",
+                                         "frac": round(dense_gbs / peak, 4), "bytes_per_cell": 25,
+                                         "peak_kind": peak_kind} if dense_gbs else None)},
+        }
+    return {
         "workload": "E: D2Q9 swimmer mix {256x128, 512x192, 1200x400}, 198-edge fish, 8 actions x 10 substeps",
         "storage": "f16",
-        "batched": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()},
+        "by_concurrency": by_c,
         "plain_f32": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in plain.items()},
-        "speedup_vs_plain": round(r["env_steps_per_s"] / plain["env_steps_per_s"], 2),
-        "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}" + (" strip" if info["strip"] else ""),
-                 "graph_builds": info["graph_builds"],
-                 "max_episodes": 2 * concurrency,
-                 "dense_ms_at_tuning": round(info["dense_ms"], 4), "cells_at_tuning": info["tuned_cells"],
-                 "dense_roofline": ({"achieved": round(dense_gbs, 1), "peak": peak, "unit": "GB/s",
-                                     "frac": round(dense_gbs / peak, 4), "bytes_per_cell": 25,
-                                     "peak_kind": peak_kind} if dense_gbs else None)},
         "seconds": round(time.perf_counter() - t0, 1),
     }
-    return out
 
 
 def run_storage_d(wl: W.Workload, storage: str, steps: int = 40, warmup: int = 5):
@@ -524,12 +544,14 @@ def run_coupled(wl: W.Workload, steps: int = 40, warmup: int = 5):
 
 
 def run_serving_line(args):
-    """`--workload E`: the serving measurement as its own JSON line."""
+    """`--workload E`: the serving measurement as its own JSON line (the
+    headline value is the concurrency-256 mix)."""
     import torch
 
     torch.cuda.set_device(0)
     r = run_serving(iterations=args.steps, warmup=args.warmup)
-    b = r["batched"]
+    c = r["by_concurrency"]["256"]
+    b = c["batched"]
     line = {
         "metric": "env_steps_per_s", "value": b["env_steps_per_s"], "unit": "env-steps/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup,
@@ -541,7 +563,7 @@ def run_serving_line(args):
         # per control step the pool uploads one 576-byte parameter row per episode
         # and reads back the 48-byte output records of all its slots
         "e2e": {"value": b["env_steps_per_s"], "unit": "env-steps/s", "h2d_bytes_per_step": 576,
-                "d2h_bytes_per_step": round(48 * r["pool"]["max_episodes"] / max(1.0, b["concurrency_mean"]), 1)},
+                "d2h_bytes_per_step": round(48 * c["pool"]["max_episodes"] / max(1.0, b["concurrency_mean"]), 1)},
         "serving": r,
     }
     print(json.dumps(line), flush=True)

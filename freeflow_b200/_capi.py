@@ -58,6 +58,7 @@ class LbmDesc(C.Structure):
         ("fluid_dx", C.c_double), ("dt", C.c_double),
         ("boundary_velocities", C.c_float * 6),
         ("storage", C.c_int), ("periodic_mask", C.c_int), ("ref_half_populations", C.c_int),
+        ("ref_2d_wall_stream", C.c_int),
     ]
 
 

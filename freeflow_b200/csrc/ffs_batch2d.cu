@@ -42,6 +42,7 @@ template <typename T> __device__ __forceinline__ GridArgs<T> episode_args(const 
     g.ncell = e.ncell;
     g.periodic = 0;
     g.half_pops = 0;
+    g.wall_stream = 0;
     g.omega = e.omega;
     g.codec = e.codec;
     g.src = static_cast<const T *>(e.mom[parity]);

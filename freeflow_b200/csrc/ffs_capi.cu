@@ -100,6 +100,7 @@ template <typename T> GridArgs<T> args(ffs_lbm *h)
     g.ncell = (uint32_t)h->ncell;
     g.periodic = h->d.periodic_mask;
     g.half_pops = h->dim == 2 ? h->d.ref_half_populations : 0;
+    g.wall_stream = h->dim == 2 ? h->d.ref_2d_wall_stream : 0;
     g.omega = h->omega;
     g.codec = h->codec;
     g.src = static_cast<const T *>(h->mom[h->cur]);
@@ -367,6 +368,8 @@ ffs_status ffs_lbm_create(const ffs_lbm_desc *desc, ffs_lbm **out)
     if (d.storage < FFS_STORAGE_F32 || d.storage > FFS_STORAGE_BF16) return fail(FFS_ERR_INVALID_ARGUMENT, "bad storage");
     if (!(d.fluid_viscosity > 0.0) || !(d.fluid_dx > 0.0) || !(d.dt > 0.0))
         return fail(FFS_ERR_INVALID_ARGUMENT, "viscosity, dx and dt must be positive");
+    if (d.ref_2d_wall_stream != 0 && d.ref_2d_wall_stream != 1)
+        return fail(FFS_ERR_INVALID_ARGUMENT, "ref_2d_wall_stream must be 0 or 1");
     ffs_lbm *h = new (std::nothrow) ffs_lbm();
     if (!h) return fail(FFS_ERR_OUT_OF_MEMORY, "host allocation failed");
     h->d = d;

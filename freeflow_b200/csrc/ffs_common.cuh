@@ -168,27 +168,55 @@ enum Storage : int { kF32 = 0, kF16 = 1, kBF16 = 2 };
 // Reduced-precision storage keeps scaled deviations from equilibrium:
 //   rho - 1,  u * su,  (pi_ab - u_a u_b) * sp
 // su and sp are powers of two, so scaling is exact; decode(encode(x)) loses
-// only the 11-bit (fp16) or 8-bit (bf16) rounding of the deviation.
+// only the 11-bit (fp16) or 8-bit (bf16) rounding of the deviation (the
+// velocity of bf16 storage is kept in binary16: StorageTraits below).
 struct Codec {
     float su, inv_su, sp, inv_sp;
 };
 
 template <typename T> struct StorageTraits;
+// to/from: one stored value of the storage type.  to_vel/from_vel: a stored
+// velocity (u * su).  FP32 and FP16 storage keep the velocity like every
+// other moment; bfloat16 storage keeps it as a binary16 bit pattern in its
+// 16-bit slot, because an 8-bit significand rounds the per-step velocity
+// changes of slow flows away (a Taylor-Green vortex at u = 0.04 changes u by
+// about 1e-5 per step, below half an ulp of u * 16 in bfloat16), while rho - 1
+// and the stress deviations keep bfloat16's range.
 template <> struct StorageTraits<float> {
     static constexpr bool kEncoded = false;
     __device__ static float to(float v) { return v; }
     __device__ static float from(float v) { return v; }
+    __device__ static float to_vel(float v) { return v; }
+    __device__ static float from_vel(float v) { return v; }
 };
 template <> struct StorageTraits<__half> {
     static constexpr bool kEncoded = true;
     __device__ static __half to(float v) { return __float2half_rn(v); }
     __device__ static float from(__half v) { return __half2float(v); }
+    __device__ static __half to_vel(float v) { return __float2half_rn(v); }
+    __device__ static float from_vel(__half v) { return __half2float(v); }
 };
 template <> struct StorageTraits<__nv_bfloat16> {
     static constexpr bool kEncoded = true;
     __device__ static __nv_bfloat16 to(float v) { return __float2bfloat16_rn(v); }
     __device__ static float from(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 to_vel(float v)
+    {
+        return __ushort_as_bfloat16(__half_as_ushort(__float2half_rn(v)));
+    }
+    __device__ static float from_vel(__nv_bfloat16 v) { return __half2float(__ushort_as_half(__bfloat16_as_ushort(v))); }
 };
+
+// Conversion of moment k of a stored vector ([rho, u_1..u_DIM, pi...]): the
+// velocity moments through to_vel/from_vel, the others through to/from.
+template <int DIM, typename T> __device__ __forceinline__ float from_storage(int k, T v)
+{
+    return (k >= 1 && k <= DIM) ? StorageTraits<T>::from_vel(v) : StorageTraits<T>::from(v);
+}
+template <int DIM, typename T> __device__ __forceinline__ T to_storage(int k, float v)
+{
+    return (k >= 1 && k <= DIM) ? StorageTraits<T>::to_vel(v) : StorageTraits<T>::to(v);
+}
 
 // Index of pi_ab in the moment vector and the (a, b) pair of each stored
 // second moment, for the encoding above.
@@ -219,51 +247,94 @@ __device__ __forceinline__ void decode_moments(float *m, const Codec &c)
     }
 }
 
-// Encode m (floats) to storage; the u used for the stress deviation is the
-// rounded one, so that decode() reproduces pi up to the deviation's rounding.
+// Stochastic rounding of the stored velocity.  With round-to-nearest, a
+// velocity whose per-step change is below half an ulp of its 11-bit
+// significand never changes in storage: a Taylor-Green vortex on 128^3 cells
+// (u ~ 0.04, relative decay 4e-5 per step) stalls that way.  Rounding up with
+// the probability given by the position between the two neighbouring binary16
+// values keeps the stored velocity unbiased, so slow changes accumulate.
+// The dither is a hash of the cell index and of the bits of the cell's new
+// density, so a cell's encoding depends only on what it stores (every kernel
+// that writes a cell gives the same bits) and changes from step to step.
+// lowbias32 (C. Wellons, "Prospecting for Hash Functions", 2018): an integer
+// mixing function with good avalanche.
+__device__ __forceinline__ uint32_t mix32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ uint32_t vel_dither(size_t idx, float rho)
+{
+    return mix32((uint32_t)idx * 0x9e3779b9u ^ (uint32_t)((uint64_t)idx >> 32) ^ __float_as_uint(rho));
+}
+// v rounded to binary16 stochastically with 10 random bits r: adding r << 3
+// to the magnitude bits of the float and truncating the 13 bits binary16
+// does not keep rounds up with probability (dropped bits) / 2^13, to within
+// 2^-10 of an ulp; values below binary16's normal range (2^-14) or at its
+// top round to nearest.
+__device__ __forceinline__ __half half_sr(float v, uint32_t r)
+{
+    const uint32_t b = __float_as_uint(v), mag = b & 0x7fffffffu;
+    if (mag < 0x38800000u || mag >= 0x47000000u) return __float2half_rn(v);
+    return __float2half_rn(__uint_as_float((b & 0x80000000u) | ((mag + (r << 3)) & ~0x1fffu)));
+}
+template <typename T> __device__ __forceinline__ T to_vel_sr(float v, uint32_t r);
+template <> __device__ __forceinline__ float to_vel_sr<float>(float v, uint32_t) { return v; }
+template <> __device__ __forceinline__ __half to_vel_sr<__half>(float v, uint32_t r) { return half_sr(v, r); }
+template <> __device__ __forceinline__ __nv_bfloat16 to_vel_sr<__nv_bfloat16>(float v, uint32_t r)
+{
+    return __ushort_as_bfloat16(__half_as_ushort(half_sr(v, r)));
+}
+
+// The stored form of moment vector m of cell idx: FP32 as is; reduced
+// storage as rho - 1, u * su (stochastically rounded) and the stress
+// deviations from the rounded u, so that decoding reproduces pi up to the
+// deviation's rounding.
 template <int DIM, typename T>
-__device__ __forceinline__ void encode_store(const float *m, T *const *planes, uint32_t idx, const Codec &c)
+__device__ __forceinline__ void encode_values(const float *m, size_t idx, const Codec &c, T *enc)
 {
     constexpr int NM = Lattice<DIM>::NM;
     if constexpr (!StorageTraits<T>::kEncoded) {
 #pragma unroll
-        for (int k = 0; k < NM; ++k) planes[k][idx] = StorageTraits<T>::to(m[k]);
+        for (int k = 0; k < NM; ++k) enc[k] = m[k];
     } else {
         float ud[DIM];
-        planes[0][idx] = StorageTraits<T>::to(m[0] - 1.0f);
+        enc[0] = StorageTraits<T>::to(m[0] - 1.0f);
+        const uint32_t h = vel_dither(idx, m[0]);
 #pragma unroll
         for (int a = 0; a < DIM; ++a) {
-            T s = StorageTraits<T>::to(m[1 + a] * c.su);
-            planes[1 + a][idx] = s;
-            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
+            const T s = to_vel_sr<T>(m[1 + a] * c.su, (h >> (10 * a)) & 0x3ffu);
+            enc[1 + a] = s;
+            ud[a] = StorageTraits<T>::from_vel(s) * c.inv_su;
         }
 #pragma unroll
         for (int k = DIM + 1; k < NM; ++k)
-            planes[k][idx] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+            enc[k] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
     }
+}
+
+// Encode m (floats) to storage at cell idx of the planes.
+template <int DIM, typename T>
+__device__ __forceinline__ void encode_store(const float *m, T *const *planes, uint32_t idx, const Codec &c)
+{
+    T enc[Lattice<DIM>::NM];
+    encode_values<DIM, T>(m, idx, c, enc);
+#pragma unroll
+    for (int k = 0; k < Lattice<DIM>::NM; ++k) planes[k][idx] = enc[k];
 }
 
 // Same as encode_store with planes[k] = base + k * stride.
 template <int DIM, typename T>
-__device__ __forceinline__ void encode_store_strided(const float *m, T *base, size_t stride, const Codec &c)
+__device__ __forceinline__ void encode_store_strided(const float *m, T *base, size_t idx, size_t stride, const Codec &c)
 {
-    constexpr int NM = Lattice<DIM>::NM;
-    if constexpr (!StorageTraits<T>::kEncoded) {
+    T enc[Lattice<DIM>::NM];
+    encode_values<DIM, T>(m, idx, c, enc);
 #pragma unroll
-        for (int k = 0; k < NM; ++k) base[k * stride] = StorageTraits<T>::to(m[k]);
-    } else {
-        float ud[DIM];
-        base[0] = StorageTraits<T>::to(m[0] - 1.0f);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-            T s = StorageTraits<T>::to(m[1 + a] * c.su);
-            base[(1 + a) * stride] = s;
-            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
-        }
-#pragma unroll
-        for (int k = DIM + 1; k < NM; ++k)
-            base[k * stride] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
-    }
+    for (int k = 0; k < Lattice<DIM>::NM; ++k) base[idx + k * stride] = enc[k];
 }
 
 // Same as encode_store with planes[k] = base + k * stride and a 32-bit index
@@ -272,43 +343,31 @@ template <int DIM, typename T>
 __device__ __forceinline__ void encode_store_idx32(const float *m, T *base, uint32_t idx, uint32_t stride,
                                                    const Codec &c)
 {
-    constexpr int NM = Lattice<DIM>::NM;
-    if constexpr (!StorageTraits<T>::kEncoded) {
+    T enc[Lattice<DIM>::NM];
+    encode_values<DIM, T>(m, idx, c, enc);
 #pragma unroll
-        for (int k = 0; k < NM; ++k) base[idx + (uint32_t)k * stride] = StorageTraits<T>::to(m[k]);
-    } else {
-        float ud[DIM];
-        base[idx] = StorageTraits<T>::to(m[0] - 1.0f);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-            T s = StorageTraits<T>::to(m[1 + a] * c.su);
-            base[idx + (uint32_t)(1 + a) * stride] = s;
-            ud[a] = StorageTraits<T>::from(s) * c.inv_su;
-        }
-#pragma unroll
-        for (int k = DIM + 1; k < NM; ++k)
-            base[idx + (uint32_t)k * stride] =
-                StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
-    }
+    for (int k = 0; k < Lattice<DIM>::NM; ++k) base[idx + (uint32_t)k * stride] = enc[k];
 }
 
-// The values encode_store writes, as they read back: m itself for FP32, the
-// decoded rounded deviations otherwise.
+// The values encode_store writes for cell idx, as they read back: m itself
+// for FP32, the decoded rounded deviations otherwise.
 template <int DIM, typename T>
-__device__ __forceinline__ void stored_values(const float *m, float *out, const Codec &c)
+__device__ __forceinline__ void stored_values(const float *m, float *out, size_t idx, const Codec &c)
 {
     constexpr int NM = Lattice<DIM>::NM;
     if constexpr (!StorageTraits<T>::kEncoded) {
 #pragma unroll
         for (int k = 0; k < NM; ++k) out[k] = m[k];
     } else {
-        out[0] = 1.0f + StorageTraits<T>::from(StorageTraits<T>::to(m[0] - 1.0f));
+        T enc[NM];
+        encode_values<DIM, T>(m, idx, c, enc);
+        out[0] = 1.0f + StorageTraits<T>::from(enc[0]);
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) out[1 + a] = StorageTraits<T>::from(StorageTraits<T>::to(m[1 + a] * c.su)) * c.inv_su;
+        for (int a = 0; a < DIM; ++a) out[1 + a] = StorageTraits<T>::from_vel(enc[1 + a]) * c.inv_su;
 #pragma unroll
         for (int k = DIM + 1; k < NM; ++k) {
             const float ua = out[1 + MomentLayout<DIM>::pa(k)], ub = out[1 + MomentLayout<DIM>::pb(k)];
-            out[k] = fmaf(StorageTraits<T>::from(StorageTraits<T>::to((m[k] - ua * ub) * c.sp)), c.inv_sp, ua * ub);
+            out[k] = fmaf(StorageTraits<T>::from(enc[k]), c.inv_sp, ua * ub);
         }
     }
 }
@@ -318,7 +377,7 @@ __device__ __forceinline__ void load_moments(float *m, const T *base, uint32_t n
 {
     constexpr int NM = Lattice<DIM>::NM;
 #pragma unroll
-    for (int k = 0; k < NM; ++k) m[k] = StorageTraits<T>::from(base[(size_t)k * ncell + idx]);
+    for (int k = 0; k < NM; ++k) m[k] = from_storage<DIM, T>(k, base[(size_t)k * ncell + idx]);
     decode_moments<DIM, T>(m, c);
 }
 
@@ -359,6 +418,8 @@ template <typename T> struct GridArgs {
     uint32_t ncell;
     int periodic;            // bit0 x, bit1 y, bit2 z wrap the pull halo (reference: clamp)
     int half_pops;           // D2Q9: round reconstructed populations to binary16 (reference tile)
+    int wall_stream;         // D2Q9: walls stream their stored moments instead of bouncing back
+                             // (the reference's 2D kernel, ffs_lbm_desc::ref_2d_wall_stream)
     float omega;
     Codec codec;
     const T *src;            // SoA: moment k of cell c at src[k * ncell + c]

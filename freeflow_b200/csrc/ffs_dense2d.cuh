@@ -12,12 +12,17 @@ struct D2 {
     static constexpr int kHX = kTX + 2, kHY = kTY + 2, kHalo = kHX * kHY;
 };
 
-// Source index of a halo cell: clamped like the reference's min/max
-// (FsiCoupling2D.cu:104-105, FsiCoupling3D.cu:106-108) or wrapped for a
-// periodic axis.  v >= -1 always; v may exceed n by a tile width.
+// Source index of a halo cell, as the reference's shared-memory fill computes
+// it (FsiCoupling2D.cu:104-105, FsiCoupling3D.cu:106-108):
+// min(n - 1, max(0, (sm - 1) + blockDim * blockIdx)).  blockDim * blockIdx is
+// unsigned, so below the grid the sum wraps to a huge unsigned value and the
+// index comes out as n - 1; above it the min clamps to n - 1.  The halo
+// therefore wraps at the low face and clamps at the high face of every axis.
+// A periodic axis wraps at both.  v >= -1 always; v may exceed n by a tile
+// width.
 __device__ __forceinline__ int halo_index(int v, int n, bool wrap)
 {
-    if (!wrap) return v < 0 ? 0 : (v >= n ? n - 1 : v);
+    if (!wrap) return (v < 0 || v >= n) ? n - 1 : v;
     if (v < 0) v += n;
     if (v >= n) v -= n;
     if (v >= n) v %= n;
@@ -59,7 +64,7 @@ __device__ __forceinline__ void dense2d_recon(const GridArgs<T> &g, const T (&ra
 {
     float m[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) m[k] = StorageTraits<T>::from(raw[k]);
+    for (int k = 0; k < 6; ++k) m[k] = from_storage<2, T>(k, raw[k]);
     decode_moments<2, T>(m, g.codec);
     Coef<2> cf;
     cf.make(m);
@@ -86,8 +91,11 @@ __device__ __forceinline__ void dense2d_update_cell(const GridArgs<T> &g, uint32
 #pragma unroll
     for (int i = 0; i < 9; ++i) pop[i] = pull(i);
     const uint32_t wm = (f8 & (kBitNearWall | kBitOutletSrc)) ? g.wallmask[idx] : 0u;
-    if (f8 & kBitNearWall) {
-        // bounce-back: f_i(x) = f_inv(i)^rec(x) when x - c_i is a wall
+    if ((f8 & kBitNearWall) && !g.wall_stream) {
+        // bounce-back: f_i(x) = f_inv(i)^rec(x) when x - c_i is a wall (with
+        // wall_stream the reference's 2D kernel is followed instead: it
+        // overwrites that value with the ordinary pull, FsiCoupling2D.cu:
+        // 171-224, since is_blocked is set only on the moving-wall path)
 #pragma unroll
         for (int i = 1; i < 9; ++i)
             if (wm & (1u << i)) pop[i] = own(L::inv(i));
@@ -108,7 +116,7 @@ __device__ __forceinline__ void dense2d_update_cell(const GridArgs<T> &g, uint32
     if (bad_state<2>(m)) atomicOr(g.status, kStatusNonFinite);
     if (f8 & kBitOutletSrc) {
         float ms[6];
-        stored_values<2, T>(m, ms, g.codec);
+        stored_values<2, T>(m, ms, idx, g.codec);
         feed_outlets<2, T>(g, idx, ms, wm);
     }
 }
@@ -126,8 +134,7 @@ __device__ __forceinline__ void dense2d_tile_loaded(const GridArgs<T> &g, int x0
     using H = Halo2<TX, TY>;
     const int tid = threadIdx.x;
 
-    // 1. reconstruct the tile + halo.  The halo index is clamped (the
-    //    reference's min/max, FsiCoupling2D.cu:104-105) or wrapped (periodic).
+    // 1. reconstruct the tile + halo (halo indices: halo_index).
 #pragma unroll
     for (int r = 0; r < H::kPer; ++r) {
         const int c = tid + r * H::kThreads;

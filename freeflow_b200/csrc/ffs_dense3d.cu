@@ -22,18 +22,22 @@
 //     in its 27 population slots instead of a reconstruction, so whatever a
 //     fluid neighbour pulls from it adds nothing; each fluid cell next to a
 //     wall then adds its own reflected populations max(0, f_inv(i)^rec(x))
-//     once, while its own plane is in shared memory.  (A fluid cell on a
-//     non-periodic domain face whose wrapped neighbour is a wall pulls from
-//     its clamped, non-wall halo instead; that pulled value is removed
-//     explicitly.)  The result is the reference's f_i(x) = max(0,
-//     f_inv(i)^rec(x)) for wall neighbours x - c_i (FsiCoupling3D.cu:209-222);
+//     once, while its own plane is in shared memory.  The result is the
+//     reference's f_i(x) = max(0, f_inv(i)^rec(x)) for wall neighbours x - c_i
+//     (FsiCoupling3D.cu:209-222), whose wall test looks at the wrapped index.
+//     The halo index is the reference's too (halo_index: it wraps at the low
+//     face and clamps at the high face of a non-periodic axis), so the halo
+//     cell and the tested cell coincide everywhere except across a high face:
+//     halo cells beyond a high face are always reconstructed, walls included
+//     (the reference pulls them when the wrapped test says fluid), and a cell
+//     whose wrapped neighbour across the face is a wall removes that pulled
+//     value explicitly (wall_fix_part);
 //   * moments are SoA planes in HBM (128 B coalesced per warp and moment);
 //     moments, flag bytes and wall masks are prefetched a plane ahead;
 //     outlets are fed by their inner neighbour in the same pass, and cells with
 //     moving-boundary links are left to the sparse link kernel (ffs_links.cu).
 #include "ffs_dense2d.cuh"
 #include "ffs_dense3d.cuh"
-#include "ffs_f2.cuh"
 
 #include <cstdlib>
 #include <map>
@@ -186,8 +190,11 @@ __device__ __forceinline__ void add_reflected(const float *buf, int c_own, uint3
             }
 }
 
-// removes from R'' the pulled populations of the wall directions in w whose
-// c_z slice is kz_sel
+// Removes from R'' the pulled populations of the wall directions in w whose
+// c_z slice is kz_sel (their source is the current plane): across a high
+// face the halo cell holds real populations, but the wrapped test found a
+// wall, so the step takes the cell's reflected population instead
+// (add_reflected).
 __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint32_t w, int kz_sel, float (&R)[10])
 {
     while (w) {
@@ -233,27 +240,33 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     };
     const uint32_t off_own = planar(c_own), off_ring = planar(c_ring);
     const uint32_t col = inside ? (uint32_t)(y * g.nx + x) : 0u;
-    // directions whose pull leaves the grid in x or y on a non-periodic axis
-    // (the halo is clamped there, so the pulled population is the cell's own)
+    // directions whose pull crosses the high x or y face of a non-periodic
+    // axis (only there can the halo cell and the wrapped test differ)
     uint32_t oor_xy = 0;
-    if (inside && ((!wx && (x == 0 || x == g.nx - 1)) || (!wy && (y == 0 || y == g.ny - 1)))) {
+    if (inside && ((!wx && x == g.nx - 1) || (!wy && y == g.ny - 1))) {
 #pragma unroll
         for (int i = 1; i < 27; ++i) {
             int cx, cy, cz;
             dir_vec<3>(i, cx, cy, cz);
-            if ((!wx && (x - cx < 0 || x - cx >= g.nx)) || (!wy && (y - cy < 0 || y - cy >= g.ny))) oor_xy |= 1u << i;
+            if ((!wx && x - cx >= g.nx) || (!wy && y - cy >= g.ny)) oor_xy |= 1u << i;
         }
     }
-    uint32_t oor_zlo = 0, oor_zhi = 0; // directions pulling from below z = 0 / above z = nz-1
+    uint32_t oor_zhi = 0; // directions pulling across z = nz-1 from above
     if (!wz) {
 #pragma unroll
         for (int i = 1; i < 27; ++i) {
             int cx, cy, cz;
             dir_vec<3>(i, cx, cy, cz);
-            if (cz == 1) oor_zlo |= 1u << i;
             if (cz == -1) oor_zhi |= 1u << i;
         }
     }
+    // halo cells beyond a high face keep their real populations even when
+    // they are walls (x and y per thread, z per plane)
+    auto beyond_hi = [&](int c) {
+        const int hx = x0 + c % kHX - 1, hy = y0 + c / kHX - 1;
+        return (!wx && hx >= g.nx) || (!wy && hy >= g.ny);
+    };
+    const bool own_hi = beyond_hi(c_own), ring_hi = beyond_hi(c_ring);
 
     float mA[10], mB[10];
     uint32_t hA = 0, hB = 0; // node types of the two halo cells (bounce-back cells get zero slots)
@@ -263,8 +276,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
             const uint32_t io = zo + off_own, ir = zo + off_ring;
 #pragma unroll
             for (int k = 0; k < 10; ++k) {
-                mA[k] = StorageTraits<T>::from(g.src[io + (uint32_t)k * g.ncell]);
-                if (has_ring) mB[k] = StorageTraits<T>::from(g.src[ir + (uint32_t)k * g.ncell]);
+                mA[k] = from_storage<3, T>(k, g.src[io + (uint32_t)k * g.ncell]);
+                if (has_ring) mB[k] = from_storage<3, T>(k, g.src[ir + (uint32_t)k * g.ncell]);
             }
             hA = g.flags[io] & kTypeMask;
             if (has_ring) hB = g.flags[ir] & kTypeMask;
@@ -273,8 +286,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
             const T *base = g.src + zo;
 #pragma unroll
             for (int k = 0; k < 10; ++k) {
-                mA[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off_own]);
-                if (has_ring) mB[k] = StorageTraits<T>::from(base[(size_t)k * g.ncell + off_ring]);
+                mA[k] = from_storage<3, T>(k, base[(size_t)k * g.ncell + off_own]);
+                if (has_ring) mB[k] = from_storage<3, T>(k, base[(size_t)k * g.ncell + off_ring]);
             }
             hA = g.flags[zo + off_own] & kTypeMask;
             if (has_ring) hB = g.flags[zo + off_ring] & kTypeMask;
@@ -285,8 +298,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         if constexpr (IDX32) return (size_t)((uint32_t)z * (uint32_t)nxy + col);
         else return (size_t)z * nxy + col;
     };
-    auto recon_cell = [&](float *buf, float *m, uint32_t type, int c) {
-        if (is_bounce_back<3>(type)) {
+    auto recon_cell = [&](float *buf, float *m, bool zero, int c) {
+        if (zero) {
 #pragma unroll
             for (int j = 0; j < 27; ++j) buf[j * kHalo + c] = 0.0f;
             return;
@@ -299,14 +312,14 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     // A ring cell feeds the tile only the 9 populations that point into it:
     // c_y = +1 from the row below (warp 0), c_y = -1 from the row above
     // (warp 1), c_x = +-1 from the columns (warp 2).  Each warp runs one
-    // uniform path that evaluates (or, for a bounce-back cell, zeroes) just
-    // those; no other slot of a ring cell is ever read.
+    // uniform path that evaluates just those; no other slot of a ring cell is
+    // ever read.
     const int ring_kind = tid < 32 ? 0 : tid < 64 ? 1 : 2;
     const float ring_sx = tid < 74 ? 1.0f : -1.0f;                 // columns: c_x of the fed populations
     const int ring_kxo = (tid < 74 ? 2 : 0) * kHalo;               // their kx plane offset
-    auto recon_ring = [&](float *buf) {
+    auto recon_ring = [&](float *buf, bool zero) {
         const int c = c_ring;
-        if (is_bounce_back<3>(hB)) {
+        if (zero) {
 #pragma unroll
             for (int kz = 0; kz < 3; ++kz)
 #pragma unroll
@@ -327,9 +340,12 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         else
             cf.populations_col(ring_sx, [&](int kz, int ky, float v) { buf[set_of(0, ky, kz) * kHalo + ring_kxo + c] = v; });
     };
-    auto recon_plane = [&](float *buf) {
-        recon_cell(buf, mA, hA, c_own);
-        if (has_ring) recon_ring(buf);
+    // plane p's halo cells; bounce-back cells get zero slots unless they lie
+    // beyond a high face
+    auto recon_plane = [&](float *buf, int p) {
+        const bool zhi = !wz && p >= g.nz;
+        recon_cell(buf, mA, is_bounce_back<3>(hA) && !(own_hi || zhi), c_own);
+        if (has_ring) recon_ring(buf, is_bounce_back<3>(hB) && !(ring_hi || zhi));
     };
     auto flag_at = [&](int z) -> uint32_t {
         return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[cell_at(z)] : 0u;
@@ -348,7 +364,7 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     // Rn receives the new c_z = +1 slice (the cell at z = p+1)
     auto plane = [&](int p, float (&Rp)[10], float (&Rc)[10]) {
         float *buf = smem + (p & 1) * kPlane;
-        recon_plane(buf);
+        recon_plane(buf, p);
         if (p < ze) load_plane(p + 1);
         const uint32_t fnn = flag_at(p + 2);
         // mask word (wall and outlet bits) of the cell at z = p+1; only cells
@@ -358,12 +374,6 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         const uint32_t wn = (upd_n && (fn & (kBitNearWall | kBitOutletSrc))) ? g.wallmask[cell_at(p + 1)] : 0u;
         __syncthreads();
         if (inside) {
-            // wall directions whose pull would leave the grid on a non-periodic
-            // axis, per destination cell: z = p-1 (c_z = -1 slice), z = p
-            // (c_z = 0), z = p+1 (c_z = +1)
-            const uint32_t oor_p = oor_xy | ((p - 1 == g.nz - 1) ? oor_zhi : 0u);
-            const uint32_t oor_c = oor_xy;
-            const uint32_t oor_n = oor_xy | ((p + 1 == 0) ? oor_zlo : 0u);
             float S[6];
             slice_sums(buf, 0, c_own, S);
             slice_add<-1>(Rp, S);
@@ -371,10 +381,12 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
             slice_add<0>(Rc, S);
             constexpr uint32_t kWall = wall_bits_mask<3>();
             if (wc & kWall) add_reflected(buf, c_own, wc & kWall, Rc);
-            // wall directions whose clamped halo source is the cell itself:
-            // remove the pulled (non-zero) value
+            // wall directions across a high face (their halo cell held real
+            // populations): remove the pulled value, per destination cell
+            // z = p-1 (c_z = -1 slice) and z = p (c_z = 0)
+            const uint32_t oor_p = oor_xy | ((p - 1 == g.nz - 1) ? oor_zhi : 0u);
             if (wp & kWall & oor_p) wall_fix_part(buf, c_own, wp & kWall & oor_p, 0, Rp);
-            if (wc & kWall & oor_c) wall_fix_part(buf, c_own, wc & kWall & oor_c, 1, Rc);
+            if (wc & kWall & oor_xy) wall_fix_part(buf, c_own, wc & kWall & oor_xy, 1, Rc);
             // the cell at z = p - 1 is complete
             const int d = p - 1;
             if (d >= zb && is_updated(fp & kTypeMask) && !(fp & kBitLink)) {
@@ -383,18 +395,18 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
                 raw_from_scaled(Rp, R);
                 collide3(R, g.omega, m);
                 if constexpr (IDX32) encode_store_idx32<3, T>(m, g.dst, idx, g.ncell, g.codec);
-                else encode_store_strided<3, T>(m, g.dst + idx, g.ncell, g.codec);
+                else encode_store_strided<3, T>(m, g.dst, (size_t)idx, g.ncell, g.codec);
                 if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
                 if (fp & kBitOutletSrc) {
                     float ms[10];
-                    stored_values<3, T>(m, ms, g.codec);
+                    stored_values<3, T>(m, ms, idx, g.codec);
                     feed_outlets<3, T>(g, idx, ms, wp);
                 }
             }
             // Rp is free: it becomes the cell at z = p + 1
             slice_sums(buf, 2, c_own, S);
             slice_init_plus(Rp, S);
-            if (wn & kWall & oor_n) wall_fix_part(buf, c_own, wn & kWall & oor_n, 2, Rp);
+            if (wn & kWall & oor_xy) wall_fix_part(buf, c_own, wn & kWall & oor_xy, 2, Rp);
         }
         fp = fc; fc = fn; fn = fnn;
         wp = wc; wc = wn;
@@ -486,306 +498,11 @@ template <typename T, int MINB> struct Dense3dLaunch {
 };
 
 
-// ---------------------------------------------------------------------------
-// Pair variant (FP32 storage): the same z-march, two planes per step.  Every
-// shared-memory slot holds the populations of one halo cell in two
-// consecutive planes as an f32x2 pair, so the reconstruction, the slice sums
-// and the partial raw moments of both planes run as packed FP32 pairs
-// (add/sub/mul/fma.rn.f32x2, each lane rounded like the scalar instruction),
-// with one LDS.64/STS.64 per population pair.  Streaming along x and y keeps
-// pairs aligned; along z, the accumulators are the destination pairs
-// (p-1, p) and (p+1, p+2) of the source pair (p, p+1): the c_z = -1 slice adds
-// to the first and the c_z = +1 slice starts the second lane by lane, and
-// only the c_z = 0 slice crosses over (its lanes go to p and p+1).  The
-// moments of the next source pair are copied to shared memory with
-// cp.async while the current pair is processed, so the prefetch holds no
-// registers.  Per destination cell the operations, and their order, are
-// those of the single-plane kernel above.
-namespace {
-
-constexpr int kStageOwn = 20 * D3::kThreads;   // 2 planes x 10 moments per tile cell
-constexpr int kStageRing = 20 * kRing;
-constexpr size_t kPairSmemBytes = (size_t)27 * kHalo * sizeof(f2) + (size_t)(kStageOwn + kStageRing) * sizeof(float);
-
-
-__device__ __forceinline__ f2 lds_clamped(const f2 *buf, int idx)
-{
-    float lo, hi;
-    f2split(buf[idx], lo, hi);
-    return f2make(fmaxf(lo, 0.0f), fmaxf(hi, 0.0f));
-}
-
-// slice_sums for both planes of the pair
-__device__ __forceinline__ void slice_sums2(const f2 *buf, int kz, int c_own, f2 *Y)
-{
-    f2 X0[3], X1[3], X2[3];
-#pragma unroll
-    for (int ky = 0; ky < 3; ++ky) {
-        const int crow = c_own - (ky - 1) * kHX;
-        const f2 fm = lds_clamped(buf, set_of(0, ky, kz) * kHalo + crow + 1);
-        const f2 f0 = lds_clamped(buf, set_of(1, ky, kz) * kHalo + crow);
-        const f2 fp = lds_clamped(buf, set_of(2, ky, kz) * kHalo + crow - 1);
-        const f2 s = fp + fm;
-        X1[ky] = fp - fm;
-        X0[ky] = f0 + s;
-        X2[ky] = s;
-    }
-    const f2 s0 = X0[2] + X0[0];
-    Y[0] = X0[1] + s0;
-    Y[1] = X0[2] - X0[0];
-    Y[2] = s0;
-    Y[3] = X1[1] + (X1[2] + X1[0]);
-    Y[4] = X1[2] - X1[0];
-    Y[5] = X2[1] + (X2[2] + X2[0]);
-}
-
-// slice_add<-1> on both lanes
-__device__ __forceinline__ void slice_add_minus2(f2 *R, const f2 *Y)
-{
-    R[0] = R[0] + Y[0]; R[2] = R[2] + Y[1]; R[5] = R[5] + Y[2]; R[1] = R[1] + Y[3]; R[7] = R[7] + Y[4];
-    R[4] = R[4] + Y[5];
-    R[3] = R[3] - Y[0]; R[6] = R[6] + Y[0]; R[8] = R[8] - Y[1]; R[9] = R[9] - Y[3];
-}
-__device__ __forceinline__ void slice_init_plus2(f2 *R, const f2 *Y)
-{
-    R[0] = Y[0]; R[2] = Y[1]; R[5] = Y[2]; R[1] = Y[3]; R[7] = Y[4]; R[4] = Y[5];
-    R[3] = Y[0]; R[6] = Y[0]; R[8] = Y[1]; R[9] = Y[3];
-}
-
-// add_reflected / wall_fix_part on one lane of the pair buffer
-__device__ __forceinline__ void add_reflected_lane(const f2 *buf, int c_own, int lane, uint32_t w, float (&R)[10])
-{
-    const float *b = reinterpret_cast<const float *>(buf);
-#pragma unroll
-    for (int kz = 0; kz < 3; ++kz)
-#pragma unroll
-        for (int ky = 0; ky < 3; ++ky)
-#pragma unroll
-            for (int kx = 0; kx < 3; ++kx) {
-                const int i = dir_index<3>(kx, ky, kz);
-                if (i == 0) continue;
-                float f = fmaxf(b[2 * (set_of(2 - kx, 2 - ky, 2 - kz) * kHalo + c_own) + lane], 0.0f);
-                f = (w & (1u << i)) ? f : 0.0f;
-                add_basis(R, kx - 1, ky - 1, kz - 1, f);
-            }
-}
-__device__ __forceinline__ void unpull_lane(const f2 *buf, int c_own, int lane, uint32_t w, int kz_sel, float (&R)[10])
-{
-    const float *b = reinterpret_cast<const float *>(buf);
-    while (w) {
-        const int i = __ffs(w) - 1;
-        w &= w - 1;
-        int cx, cy, cz;
-        dir_vec<3>(i, cx, cy, cz);
-        if (cz + 1 != kz_sel) continue;
-        const float pulled = fmaxf(b[2 * (set_of(cx + 1, cy + 1, cz + 1) * kHalo + c_own - cx - cy * kHX) + lane], 0.0f);
-        add_basis_rt(R, cx, cy, cz, -pulled);
-    }
-}
-
-__device__ __forceinline__ void split10(const f2 *A, float (&lo)[10], float (&hi)[10])
-{
-#pragma unroll
-    for (int k = 0; k < 10; ++k) f2split(A[k], lo[k], hi[k]);
-}
-__device__ __forceinline__ void join10(f2 *A, const float (&lo)[10], const float (&hi)[10])
-{
-#pragma unroll
-    for (int k = 0; k < 10; ++k) A[k] = f2make(lo[k], hi[k]);
-}
-
-} // namespace
-
-template <int MINB>
-__global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_pair_kernel(GridArgs<float> g, int zchunk)
-{
-    extern __shared__ float4 smem4[];
-    f2 *pops = reinterpret_cast<f2 *>(smem4);
-    float *stage = reinterpret_cast<float *>(pops + 27 * kHalo);
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
-    const int zb = blockIdx.z * zchunk;
-    const int ze = min(zb + zchunk, g.nz);
-    const long long nxy = (long long)g.nx * g.ny;
-    const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
-
-    const int tx = tid % kTX, ty = tid / kTX;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool inside = x < g.nx && y < g.ny;
-    const int c_own = (ty + 1) * kHX + (tx + 1);
-    const bool has_ring = tid < kRing;
-    const int c_ring = has_ring ? ring_cell(tid) : c_own;
-    auto planar = [&](int c) {
-        int hx = c % kHX, hy = c / kHX;
-        return (uint32_t)(halo_index(y0 + hy - 1, g.ny, wy) * g.nx + halo_index(x0 + hx - 1, g.nx, wx));
-    };
-    const uint32_t off_own = planar(c_own), off_ring = planar(c_ring);
-    const uint32_t col = inside ? (uint32_t)(y * g.nx + x) : 0u;
-    uint32_t oor_xy = 0;
-    if (inside && ((!wx && (x == 0 || x == g.nx - 1)) || (!wy && (y == 0 || y == g.ny - 1)))) {
-#pragma unroll
-        for (int i = 1; i < 27; ++i) {
-            int cx, cy, cz;
-            dir_vec<3>(i, cx, cy, cz);
-            if ((!wx && (x - cx < 0 || x - cx >= g.nx)) || (!wy && (y - cy < 0 || y - cy >= g.ny))) oor_xy |= 1u << i;
-        }
-    }
-    uint32_t oor_zlo = 0, oor_zhi = 0;
-    if (!wz) {
-#pragma unroll
-        for (int i = 1; i < 27; ++i) {
-            int cx, cy, cz;
-            dir_vec<3>(i, cx, cy, cz);
-            if (cz == 1) oor_zlo |= 1u << i;
-            if (cz == -1) oor_zhi |= 1u << i;
-        }
-    }
-    constexpr uint32_t kWall = wall_bits_mask<3>();
-
-    // moments of source planes (s, s+1) -> stage (cp.async), node types -> registers
-    float *st_own = stage + tid;
-    float *st_ring = stage + kStageOwn + tid;
-    uint32_t types = 0; // own lo | own hi << 8 | ring lo << 16 | ring hi << 24
-    auto issue_pair = [&](int s) {
-        uint32_t ty4 = 0;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const size_t zo = (size_t)halo_index(s + h, g.nz, wz) * nxy;
-            const float *base = g.src + zo;
-#pragma unroll
-            for (int k = 0; k < 10; ++k) {
-                cp_async4(st_own + (h * 10 + k) * D3::kThreads, base + (size_t)k * g.ncell + off_own);
-                if (has_ring) cp_async4(st_ring + (h * 10 + k) * kRing, base + (size_t)k * g.ncell + off_ring);
-            }
-            ty4 |= (uint32_t)(g.flags[zo + off_own] & kTypeMask) << (8 * h);
-            if (has_ring) ty4 |= (uint32_t)(g.flags[zo + off_ring] & kTypeMask) << (16 + 8 * h);
-        }
-        cp_async_commit();
-        return ty4;
-    };
-    // reconstructs the pair of one halo cell; a bounce-back lane gets zeros
-    auto recon_pair = [&](const float *st, int stride, uint32_t tlo, uint32_t thi, int c) {
-        const bool zlo = is_bounce_back<3>(tlo), zhi = is_bounce_back<3>(thi);
-        f2 m[10];
-#pragma unroll
-        for (int k = 0; k < 10; ++k) {
-            const float lo = zlo ? 0.0f : st[k * stride], hi = zhi ? 0.0f : st[(10 + k) * stride];
-            m[k] = f2make(lo, hi);
-        }
-        Coef3V<f2> cf;
-        cf.make(m);
-        cf.populations_each([&](int kz, int ky, int kx, f2 v) { pops[set_of(kx, ky, kz) * kHalo + c] = v; });
-    };
-    auto flag_at = [&](int z) -> uint32_t {
-        return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[(size_t)z * nxy + col] : 0u;
-    };
-    auto mask_at = [&](int z, uint32_t f) -> uint32_t {
-        const bool upd = is_updated(f & kTypeMask) && !(f & kBitLink);
-        return (upd && (f & (kBitNearWall | kBitOutletSrc))) ? g.wallmask[(size_t)z * nxy + col] : 0u;
-    };
-    auto finish = [&](int d, uint32_t f, uint32_t w, const float (&R)[10]) {
-        if (d < zb || d >= ze || !is_updated(f & kTypeMask) || (f & kBitLink)) return;
-        const uint32_t idx = (uint32_t)(d * nxy + col);
-        float m[10];
-        collide3(R, g.omega, m);
-        encode_store_strided<3, float>(m, g.dst + idx, g.ncell, g.codec);
-        if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
-        if (f & kBitOutletSrc) feed_outlets<3, float>(g, idx, m, w);
-    };
-
-    // flags and masks of the destination planes s-1, s, s+1, s+2 of source pair (s, s+1)
-    uint32_t fl0 = 0, fl1 = 0, fl2 = flag_at(zb), fl3 = flag_at(zb + 1);
-    uint32_t wm0 = 0, wm1 = 0;
-    f2 A[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) A[k] = f2make(0.0f, 0.0f);
-    types = issue_pair(zb - 1);
-    for (int s = zb - 1; s <= ze; s += 2) {
-        cp_async_wait<0>();
-        recon_pair(st_own, D3::kThreads, types & 0xFF, (types >> 8) & 0xFF, c_own);
-        if (has_ring) recon_pair(st_ring, kRing, (types >> 16) & 0xFF, types >> 24, c_ring);
-        // the next pair's moments and types, the flags two planes ahead, this pair's masks
-        if (s + 2 <= ze) types = issue_pair(s + 2);
-        const uint32_t fl4 = flag_at(s + 3), fl5 = flag_at(s + 4);
-        const uint32_t wm2 = mask_at(s + 1, fl2), wm3 = mask_at(s + 2, fl3);
-        __syncthreads();
-        if (inside) {
-            const uint32_t oor_d0 = oor_xy | ((s - 1 == g.nz - 1) ? oor_zhi : 0u); // dest s-1, c_z = -1
-            const uint32_t oor_d1 = oor_xy | ((s == g.nz - 1) ? oor_zhi : 0u);     // dest s,   c_z = -1
-            const uint32_t oor_d2 = oor_xy | ((s + 1 == 0) ? oor_zlo : 0u);        // dest s+1, c_z = +1
-            const uint32_t oor_d3 = oor_xy | ((s + 2 == 0) ? oor_zlo : 0u);        // dest s+2, c_z = +1
-            f2 S0[6], S[6];
-            slice_sums2(pops, 1, c_own, S0);
-            float alo[10], ahi[10];
-            split10(A, alo, ahi);
-            float s0lo[6], s0hi[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) f2split(S0[k], s0lo[k], s0hi[k]);
-            // dest s (lane hi of A): c_z = 0 slice from source s (lane lo)
-            ahi[0] += s0lo[0]; ahi[2] += s0lo[1]; ahi[5] += s0lo[2]; ahi[1] += s0lo[3]; ahi[7] += s0lo[4];
-            ahi[4] += s0lo[5];
-            if (wm1 & kWall) add_reflected_lane(pops, c_own, 0, wm1 & kWall, ahi);
-            if (wm1 & kWall & oor_xy) unpull_lane(pops, c_own, 0, wm1 & kWall & oor_xy, 1, ahi);
-            join10(A, alo, ahi);
-            // c_z = -1 slice: source s -> dest s-1 (lo), source s+1 -> dest s (hi)
-            slice_sums2(pops, 0, c_own, S);
-            slice_add_minus2(A, S);
-            if (((wm0 & oor_d0) | (wm1 & oor_d1)) & kWall) {
-                split10(A, alo, ahi);
-                if (wm0 & kWall & oor_d0) unpull_lane(pops, c_own, 0, wm0 & kWall & oor_d0, 0, alo);
-                if (wm1 & kWall & oor_d1) unpull_lane(pops, c_own, 1, wm1 & kWall & oor_d1, 0, ahi);
-                join10(A, alo, ahi);
-            }
-            // destinations s-1 and s are complete
-            split10(A, alo, ahi);
-            finish(s - 1, fl0, wm0, alo);
-            finish(s, fl1, wm1, ahi);
-            // c_z = +1 slice starts dest s+1 (lo, from source s) and s+2 (hi, from source s+1)
-            slice_sums2(pops, 2, c_own, S);
-            slice_init_plus2(A, S);
-            split10(A, alo, ahi);
-            if (wm2 & kWall & oor_d2) unpull_lane(pops, c_own, 0, wm2 & kWall & oor_d2, 2, alo);
-            if (wm3 & kWall & oor_d3) unpull_lane(pops, c_own, 1, wm3 & kWall & oor_d3, 2, ahi);
-            // dest s+1 (lane lo): c_z = 0 slice from source s+1 (lane hi), own reflected populations
-            alo[0] += s0hi[0]; alo[2] += s0hi[1]; alo[5] += s0hi[2]; alo[1] += s0hi[3]; alo[7] += s0hi[4];
-            alo[4] += s0hi[5];
-            if (wm2 & kWall) add_reflected_lane(pops, c_own, 1, wm2 & kWall, alo);
-            if (wm2 & kWall & oor_xy) unpull_lane(pops, c_own, 1, wm2 & kWall & oor_xy, 1, alo);
-            join10(A, alo, ahi);
-        }
-        fl0 = fl2; fl1 = fl3; fl2 = fl4; fl3 = fl5;
-        wm0 = wm2; wm1 = wm3;
-        __syncthreads(); // every pull of this pair is done before the next reconstruction
-    }
-}
-
-template <int MINB> struct Dense3dPairLaunch {
-    static cudaError_t run(const GridArgs<float> &g, cudaStream_t s)
-    {
-        int slots = 0;
-        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_pair_kernel<MINB>), D3::kThreads,
-                                       kPairSmemBytes, slots);
-        if (e != cudaSuccess) return e;
-        int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY;
-        int nchunk = choose_zchunks(tx * ty, g.nz, slots);
-        int zchunk = (g.nz + nchunk - 1) / nchunk;
-        dim3 grid(tx, ty, (g.nz + zchunk - 1) / zchunk);
-        dense3d_pair_kernel<MINB><<<grid, D3::kThreads, kPairSmemBytes, s>>>(g, zchunk);
-        return cudaGetLastError();
-    }
-};
-
-template <typename T> bool dense3d_has_variant(int v)
-{
-    return v == 2 ? std::is_same<T, float>::value : (v >= 0 && v < kDense3dVariants);
-}
+template <typename T> bool dense3d_has_variant(int v) { return v >= 0 && v < kDense3dVariants; }
 
 template <typename T>
 cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
 {
-    if constexpr (std::is_same<T, float>::value) {
-        if (variant == 2) return Dense3dPairLaunch<2>::run(g, s);
-    }
     return variant == 1 ? Dense3dLaunch<T, 3>::run(g, s) : Dense3dLaunch<T, 2>::run(g, s);
 }
 
@@ -804,10 +521,9 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     cudaEventCreate(&b);
     float best = 1e30f;
     int best_v = 0;
-    // only the variants that round identically take part: the single-plane
-    // kernel for two and three CTAs per SM (the pair kernel orders its
-    // floating-point operations differently and runs only when pinned)
-    for (int v = 0; v < 2; ++v) {
+    // the single-plane kernel for two and three CTAs per SM, which round
+    // identically
+    for (int v = 0; v < kDense3dVariants; ++v) {
         if (!dense3d_has_variant<T>(v)) continue;
         if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue; // warm-up
         cudaEventRecord(a, s);

@@ -13,11 +13,10 @@ struct D3 {
 };
 static_assert(D3::kRing <= D3::kThreads, "every ring cell needs a partner thread");
 
-// variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM, 2 = the
-// pair kernel (two planes per step in f32x2; FP32 storage only).  The first
-// step times 0 and 1, which round identically, and keeps the faster; 2 runs
-// only when pinned with FFS_DENSE3D_VARIANT.
-constexpr int kDense3dVariants = 3;
+// variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM.  Both
+// round identically; the first step times them and keeps the faster
+// (FFS_DENSE3D_VARIANT pins one).
+constexpr int kDense3dVariants = 2;
 template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant);
 template <typename T> int tune_dense3d(const GridArgs<T> &g, cudaStream_t s);
 

@@ -200,12 +200,15 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
             const int ax = (x1 + g.nx) % g.nx, ay = (y1 + g.ny) % g.ny, az = (z1 + g.nz) % g.nz;
             const uint32_t ib = (uint32_t)((long long)az * nxy + (long long)ay * g.nx + ax);
             bool done = false;
-            if (is_bounce_back<DIM>(g.flags[ib] & kTypeMask)) {
+            // a wall neighbour: bounce-back, no link (with wall_stream in 2D, the
+            // reference's 2D kernel: the ordinary pull, no link either)
+            const bool bb = is_bounce_back<DIM>(g.flags[ib] & kTypeMask);
+            if (bb && !(DIM == 2 && g.wall_stream)) {
                 float v = own.population(-cx, -cy, -cz);
                 if (HALF) v = round_half(v);
                 pop = fmaxf(v, 0.0f);
                 done = true;
-            } else if (notCross) {
+            } else if (!bb && notCross) {
                 const unsigned long long key = links[(size_t)slot * Q + i];
                 if (key != ~0ull) {
                     const uint32_t e = (uint32_t)(key & 0xffffffffull);
@@ -265,7 +268,7 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
                 }
             }
             if (!done) {
-                // ordinary pull from the (clamped or wrapped) upstream cell
+                // ordinary pull from the upstream halo cell (halo_index)
                 const int sx = halo_index(x1, g.nx, wx), sy = halo_index(y1, g.ny, wy), sz = halo_index(z1, g.nz, wz);
                 const uint32_t sidx = (uint32_t)((long long)sz * nxy + (long long)sy * g.nx + sx);
                 float mn[NM];
@@ -310,7 +313,7 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
             if (bad_state<DIM>(m)) atomicOr(g.status, kStatusNonFinite);
             if (f8 & kBitOutletSrc) {
                 float ms[NM];
-                stored_values<DIM, T>(m, ms, g.codec);
+                stored_values<DIM, T>(m, ms, cell, g.codec);
                 feed_outlets<DIM, T>(g, cell, ms, g.wallmask[cell]);
             }
         }

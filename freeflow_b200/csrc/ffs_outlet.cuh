@@ -113,7 +113,7 @@ __device__ __forceinline__ void feed_outlets(const GridArgs<T> &g, uint32_t p, c
                 if (k == rule.comp && outward) mq[k] = up;
                 if (k == rule.pcomp) mq[k] = up * up;
             }
-            encode_store_strided<DIM, T>(mq, g.dst + q, g.ncell, g.codec);
+            encode_store_strided<DIM, T>(mq, g.dst, q, g.ncell, g.codec);
         }
     }
 }

@@ -155,7 +155,7 @@ class FluidGrid:
     def __init__(self, dim: int, nx: int, ny: int, nz: int = 1, fluid_viscosity: float = 0.001,
                  fluid_density: float = 1000.0, fluid_dx: float = 1.0, dt: float = 0.001,
                  boundary_velocities=None, storage: str = "f32", periodic: int = 0,
-                 ref_half_populations: bool = False):
+                 ref_half_populations: bool = False, ref_2d_wall_stream: bool = False):
         L = A.load()
         d = A.LbmDesc()
         d.dim, d.nx, d.ny, d.nz = dim, nx, ny, (1 if dim == 2 else nz)
@@ -166,6 +166,7 @@ class FluidGrid:
         d.storage = A.STORAGE[storage] if isinstance(storage, str) else int(storage)
         d.periodic_mask = int(periodic)
         d.ref_half_populations = int(bool(ref_half_populations))
+        d.ref_2d_wall_stream = int(bool(ref_2d_wall_stream))
         self._h = C.c_void_p()
         A.check(L.ffs_lbm_create(C.byref(d), C.byref(self._h)), "ffs_lbm_create")
         self.dim, self.nx, self.ny, self.nz = dim, nx, ny, d.nz

@@ -401,29 +401,39 @@ def serve(pool: Pool, specs: list[EpisodeSpec], iterations: int, initial: int, a
     }
 
 
-def plain_rate(specs: list[EpisodeSpec], control_steps: int, substeps: int = 10) -> dict:
+def plain_rate(specs: list[EpisodeSpec], control_steps: int, substeps: int = 10, min_seconds: float = 0.0) -> dict:
     """Plain per-episode path over `specs`, one episode at a time: env-steps/s
-    and per-step latency percentiles (each control step ends with a host sync)."""
+    and per-step latency percentiles (each control step ends with a host sync).
+
+    Each episode runs at least `control_steps` control steps and at least
+    `min_seconds` of timed control steps.  The rate weights every spec equally
+    (the mix of the batched path draws its grid sizes uniformly): one env-step
+    of the mix costs the mean, over the specs, of their mean step times."""
     import torch
 
     lat = []
+    per_spec = []
     t0 = time.perf_counter()
-    n = 0
     for sp in specs:
         env = PlainEnv(sp)
         rng = np.random.default_rng(sp.seed)
         env.set_action(rng.uniform(-1.0, 1.0, 8).astype(np.float32))
         env.control_step(substeps)  # warm: first-step set-up of this grid
         torch.cuda.synchronize()
-        for _ in range(control_steps):
+        mine = []
+        while len(mine) < control_steps or sum(mine) < min_seconds:
             a = time.perf_counter()
             env.set_action(rng.uniform(-1.0, 1.0, 8).astype(np.float32))
             env.control_step(substeps)
-            lat.append(time.perf_counter() - a)
-            n += 1
+            mine.append(time.perf_counter() - a)
         env.close()
-    wall = sum(lat)
+        lat.extend(mine)
+        per_spec.append({"grid": f"{sp.nx}x{sp.ny}", "env_steps": len(mine), "seconds": round(sum(mine), 3),
+                         "env_steps_per_s": round(len(mine) / sum(mine), 1),
+                         "p50_ms": round(float(np.percentile(np.array(mine) * 1e3, 50)), 4)})
+    mean_step = float(np.mean([s["seconds"] / s["env_steps"] for s in per_spec]))
     lat_ms = np.array(lat) * 1e3
-    return {"env_steps": n, "seconds": wall, "env_steps_per_s": n / wall if wall > 0 else 0.0,
+    return {"env_steps": len(lat), "seconds": float(sum(lat)),
+            "env_steps_per_s": 1.0 / mean_step if mean_step > 0 else 0.0,
             "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-            "wall_including_setup_s": time.perf_counter() - t0}
+            "per_grid": per_spec, "wall_including_setup_s": time.perf_counter() - t0}

@@ -56,11 +56,11 @@ class Workload:
             return self.rest.astype(np.float32), np.zeros_like(self.rest, dtype=np.float32)
         return self.kinematics(step * self.dt)
 
-    def grid_kwargs(self, storage="f32", ref_half_populations=False):
+    def grid_kwargs(self, storage="f32", ref_half_populations=False, ref_2d_wall_stream=False):
         return dict(dim=self.dim, nx=self.nx, ny=self.ny, nz=self.nz, fluid_viscosity=self.fluid_viscosity,
                     fluid_density=self.fluid_density, fluid_dx=self.fluid_dx, dt=self.dt,
                     boundary_velocities=self.boundary_velocities, storage=storage, periodic=self.periodic,
-                    ref_half_populations=ref_half_populations)
+                    ref_half_populations=ref_half_populations, ref_2d_wall_stream=ref_2d_wall_stream)
 
 
 def equilibrium_moments(rho, u, dtype=np.float32):

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define FFS_ABI_VERSION 3
+#define FFS_ABI_VERSION 4
 
 typedef struct ffs_lbm ffs_lbm;
 
@@ -71,11 +71,22 @@ typedef struct {
     double dt;
     float boundary_velocities[6];  /* [vx_left, vy_down, vx_right, vy_up(, v_front, v_back)] */
     int storage;                   /* ffs_storage */
-    int periodic_mask;             /* bit0 x, bit1 y, bit2 z: wrap the streaming halo.
-                                      0 = the reference's clamped halo */
+    int periodic_mask;             /* bit0 x, bit1 y, bit2 z: wrap the streaming halo at
+                                      both faces.  0 = the reference's halo, which
+                                      wraps at the low face and clamps at the high
+                                      face of each axis (FsiCoupling2D.cu:104-105,
+                                      FsiCoupling3D.cu:106-108: unsigned index
+                                      arithmetic); the bounce-back test always uses
+                                      the wrapped neighbour (:163-176, :200-216) */
     int ref_half_populations;      /* D2Q9 only: round reconstructed populations to
                                       binary16 as the reference's __half tile does
                                       (FsiCoupling2D.cu:89,120-128) */
+    int ref_2d_wall_stream;        /* D2Q9 only: 1 = walls stream their stored moments
+                                      as in the reference's 2D kernel, which computes
+                                      the bounce-back value and then overwrites it with
+                                      the ordinary pull (FsiCoupling2D.cu:171-224:
+                                      is_blocked is set only on the moving-wall path);
+                                      0 = bounce-back, as the 3D kernel does */
 } ffs_lbm_desc;
 
 /* Surface seen by the fluid step; mirrors SolidGeometryProxy_Device<DIM>

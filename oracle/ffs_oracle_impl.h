@@ -44,8 +44,9 @@
 typedef struct {
     int dim, nx, ny, nz, Q, NM;
     long long ncell;
-    int periodic;   /* bit0 x, bit1 y, bit2 z: halo wraps instead of clamping */
+    int periodic;   /* bit0 x, bit1 y, bit2 z: halo wraps at both faces */
     int half_pops;  /* D2Q9: round the reconstructed tile to binary16 (reference smem) */
+    int wall_stream;/* D2Q9: walls stream their moments (the reference's 2D kernel) */
     R vis, cl, ct, cf, omega;
     float clf;      /* lattice spacing as the reference's float (link geometry) */
     float bcvel[6];
@@ -376,7 +377,12 @@ static inline void FN(dirs)(const FN(grid) *g, const int **ex, const int **ey, c
     else { *ex = FN(ex3); *ey = FN(ey3); *ez = FN(ez3); *inv = FN(inv3); }
 }
 
-static inline int FN(clampi)(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+/* Halo index of a non-periodic axis as the reference's shared-memory fill
+ * forms it (FsiCoupling2D.cu:104-105, FsiCoupling3D.cu:106-108):
+ * min(n - 1, max(0, (s - 1) + blockDim * blockIdx)) with an unsigned
+ * blockDim * blockIdx, so -1 becomes a huge unsigned value and then n - 1
+ * (the low face wraps) while n is clamped to n - 1 (the high face clamps). */
+static inline int FN(haloi)(int v, int n) { return (v < 0 || v >= n) ? n - 1 : v; }
 static inline int FN(wrapi)(int v, int n) { return ((v % n) + n) % n; }
 
 /* ------------------------------------------------------------- life cycle */
@@ -392,7 +398,10 @@ FN(grid) *FN(create)(int dim, int nx, int ny, int nz, double viscosity, double d
     g->dim = dim; g->nx = nx; g->ny = ny; g->nz = nz;
     g->Q = dim == 2 ? 9 : 27; g->NM = dim == 2 ? 6 : 10;
     g->ncell = (long long)nx * ny * nz;
-    g->periodic = periodic; g->half_pops = (dim == 2) ? half_pops : 0;
+    /* half_pops bit 0: binary16 tile; bit 1: 2D walls stream (both 2D only) */
+    g->periodic = periodic;
+    g->half_pops = (dim == 2) ? (half_pops & 1) : 0;
+    g->wall_stream = (dim == 2) ? ((half_pops >> 1) & 1) : 0;
     /* m_viscosity is a float (LbmFlowField2D.hpp:177); omega is formed in double
      * (FsiCoupling2D.cu:236, FsiCoupling3D.cu:303) and rounded to R. */
     float visf = (float)viscosity;
@@ -600,13 +609,17 @@ static void FN(update_cell)(FN(grid) *g, const R *src, R *dst, int x, int y, int
         int notCross = x1 >= 0 && x1 < nx && y1 >= 0 && y1 < ny && z1 >= 0 && z1 < nz;
         int wx = FN(wrapi)(x1, nx), wy = FN(wrapi)(y1, ny), wz = FN(wrapi)(z1, nz);
         long long ib = ((long long)wz * ny + wy) * nx + wx;
-        if (FN(is_bb)(dim, g->flags[ib])) {
+        const int bb = FN(is_bb)(dim, g->flags[ib]);
+        if (bb && !(dim == 2 && g->wall_stream)) {
             R v = own[inv[i]];
             pop[i] = v > 0 ? v : (R)0;
             continue;
         }
+        /* wall_stream, 2D: the reference's kernel computes the bounce-back value
+         * but, is_blocked being set only on the moving-wall path, overwrites it
+         * with the ordinary pull and skips the link (FsiCoupling2D.cu:171-224) */
         int blocked = 0;
-        if (with_links && notCross) {
+        if (with_links && notCross && !bb) {
             long long li = FN(find_link)(g, (uint64_t)cid * Q + i);
             if (li >= 0) {
                 int e = (int)(g->link_key[li] & 0xFFFFFFFFu);
@@ -677,8 +690,8 @@ static void FN(update_cell)(FN(grid) *g, const R *src, R *dst, int x, int y, int
         }
         if (!blocked) {
             int sx, sy, sz;
-            if (g->periodic & 1) sx = wx; else sx = FN(clampi)(x1, nx);
-            if (g->periodic & 2) sy = wy; else sy = FN(clampi)(y1, ny);
+            if (g->periodic & 1) sx = wx; else sx = FN(haloi)(x1, nx);
+            if (g->periodic & 2) sy = wy; else sy = FN(haloi)(y1, ny);
             (void)sz;
             const R *pl = P[1 - cz]; /* plane z - cz */
             R v = pl[((size_t)sy * nx + sx) * Q + i];
@@ -850,7 +863,7 @@ static void FN(zset)(const FN(grid) *g, int z, int *zs)
         int zz = z - 1 + k;
         if (g->dim == 2) zz = 0;
         else if (g->periodic & 4) zz = FN(wrapi)(zz, g->nz);
-        else zz = FN(clampi)(zz, g->nz);
+        else zz = FN(haloi)(zz, g->nz);
         zs[k] = zz;
     }
 }

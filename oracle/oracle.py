@@ -10,8 +10,9 @@ Two builds of the same restatement are exposed:
   ``half_pops=True``);
 * ``Oracle(..., precision="phys64")`` runs the same update in FP64.
 
-Parity against the reference itself is unpinned (the reference ships no golden
-vectors and cannot be built here); see ``ffs_oracle_impl.h``.
+The restatement is pinned to the reference's own step: ``ref.py`` runs the
+reference's unmodified CUDA sources (built into ``_ref/`` by ``make ref``) on
+the GPU, and the GPU tests compare this oracle and the product against it.
 """
 from __future__ import annotations
 
@@ -138,7 +139,7 @@ class Oracle:
     """
 
     def __init__(self, dim, nx, ny, nz=1, viscosity=0.01, density=1000.0, dx=1.0, dt=1.0,
-                 boundary_velocities=None, periodic=0, half_pops=False, precision="ref32"):
+                 boundary_velocities=None, periodic=0, half_pops=False, precision="ref32", wall_stream=False):
         self.dim, self.nx, self.ny = dim, nx, ny
         self.nz = 1 if dim == 2 else nz
         self.nm = 6 if dim == 2 else 10
@@ -150,7 +151,8 @@ class Oracle:
             bc[: len(v)] = v
         L = lib()
         self._h = getattr(L, self.pre + "create")(dim, nx, ny, self.nz, viscosity, density, dx, dt,
-                                                  _ptr(bc), int(periodic), int(half_pops))
+                                                  _ptr(bc), int(periodic),
+                                                  int(bool(half_pops)) | (int(bool(wall_stream)) << 1))
         if not self._h:
             raise ValueError("invalid grid description")
 

@@ -7,10 +7,10 @@ import numpy as np
 from freeflow_b200 import workloads as W
 
 
-def make_gpu(wl: W.Workload, storage="f32", ref_half=False, periodic=None):
+def make_gpu(wl: W.Workload, storage="f32", ref_half=False, periodic=None, wall_stream=False):
     from freeflow_b200 import DeviceSurface, FluidGrid
 
-    kw = wl.grid_kwargs(storage=storage, ref_half_populations=ref_half)
+    kw = wl.grid_kwargs(storage=storage, ref_half_populations=ref_half, ref_2d_wall_stream=wall_stream)
     if periodic is not None:
         kw["periodic"] = periodic
     g = FluidGrid(**kw)
@@ -23,12 +23,13 @@ def make_gpu(wl: W.Workload, storage="f32", ref_half=False, periodic=None):
     return g, surf
 
 
-def make_oracle(wl: W.Workload, precision="ref32", half_pops=False, periodic=None):
+def make_oracle(wl: W.Workload, precision="ref32", half_pops=False, periodic=None, wall_stream=False):
     from oracle.oracle import Oracle
 
     o = Oracle(wl.dim, wl.nx, wl.ny, wl.nz, viscosity=wl.fluid_viscosity, density=wl.fluid_density,
                dx=wl.fluid_dx, dt=wl.dt, boundary_velocities=wl.boundary_velocities,
-               periodic=wl.periodic if periodic is None else periodic, half_pops=half_pops, precision=precision)
+               periodic=wl.periodic if periodic is None else periodic, half_pops=half_pops, precision=precision,
+               wall_stream=wall_stream)
     o.set_flags(wl.flags)
     o.set_moments(wl.moments.astype(np.float64))
     return o

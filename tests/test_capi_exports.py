@@ -36,7 +36,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_status_strings():
     L = _capi.load()
-    assert L.ffs_abi_version() == 3
+    assert L.ffs_abi_version() == 4
     assert L.ffs_status_string(0) == b"ok"
     assert L.ffs_status_string(1) == b"invalid argument"
 

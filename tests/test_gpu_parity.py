@@ -130,8 +130,9 @@ def test_3d_taylor_green_periodic_vs_fp64(cuda):
     assert max_abs(gm, om) <= 5e-6
 
 
-def test_3d_clamped_halo_reference_mode(cuda):
-    """Reference semantics without periodicity: the halo is clamped (quirk Q1)."""
+def test_3d_reference_halo_without_periodicity(cuda):
+    """Reference semantics without periodicity: the halo wraps at the low face
+    and clamps at the high face of each axis (FsiCoupling3D.cu:106-108)."""
     wl = W.taylor_green_3d(n=20, u0=0.04, viscosity=0.01)
     gm, om, _, _, st = run_pair(wl, 8, periodic=0)
     assert st == 0
@@ -150,8 +151,9 @@ def test_3d_walls_inlet_outlet_channel(cuda):
 
 def test_3d_open_face_with_wall_across_the_wrap(cuda):
     """Fluid cells on a non-periodic face whose wrapped neighbour is a wall:
-    the reference bounces back (wall test on the wrapped index) although its
-    halo pull is clamped to the cell itself (FsiCoupling3D.cu:106-108 vs
+    the reference bounces back (wall test on the wrapped index).  At a low
+    face the halo wraps too, at a high face it is clamped to the face, so
+    there the pulled value must be replaced (FsiCoupling3D.cu:106-108 vs
     :203-216)."""
     wl = W.taylor_green_3d(n=20, u0=0.03, viscosity=0.01)
     f = wl.flags.reshape(20, 20, 20)
