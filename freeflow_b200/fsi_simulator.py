@@ -26,8 +26,9 @@ Scope is the fluid step.
   ``getBoundaryPointIdx`` the surface, its elements and its vertex map.
 - The ``"static"`` solid solver is mirrored: a rigid body moved by ``apply_kinematic_control``
   (``src/fem/StaticBodySolver.cpp:122-151``).
-- The deformable solvers (``"vbd"``, Newton) and LBS control are outside this package. A caller
-  that owns a solid model sets the volume vertices with ``set_surface`` instead.
+- The deformable solvers (``"vbd"``, Newton) and LBS control are outside this package. A
+  configuration that names one loads and steps with a warning; the solid keeps its placed rest shape
+  until a caller that owns a solid model sets the volume vertices with ``set_surface``.
 
 Differences from the reference that a caller can see:
 
@@ -226,6 +227,8 @@ def params_from_json(j: dict, dim: int):
     _fill(p, j, keys)
     if dim == 2 and "boundary_velocities" not in j:
         p.boundary_velocities = [0.0] * 4
+    # std::vector<float> in the reference: the values pass through float
+    p.boundary_velocities = [float(np.float32(v)) for v in p.boundary_velocities]
     if isinstance(j.get("global_fem_options"), dict):
         _fill(p.global_fem_options, j["global_fem_options"], list(FemSolverOptions.__dataclass_fields__))
     for bc in j.get("boundaries", []) or []:
@@ -373,8 +376,10 @@ class _SimulatorBase:
 
         p = self.m_params
         if p.solid_solver_type not in ("static",):
-            raise ValueError(f"solid_solver_type '{p.solid_solver_type}': only the static (kinematic) solid is part of "
-                             "this package; drive a deformable solid through set_surface()")
+            # a configuration written for a deformable solver (fish2d_lbs_control.json: "vbd") still
+            # loads and steps: the solid keeps its placed rest shape until its owner sets the vertices
+            warnings.warn(f"solid_solver_type '{p.solid_solver_type}': the deformable solid solvers are not part "
+                          "of this package; the solid keeps its rest shape until set_surface() moves it")
         bc = list(p.boundary_velocities)
         if len(bc) != 2 * self.DIM:
             bc = [0.0] * (2 * self.DIM)

@@ -32,7 +32,7 @@ def test_config2d_fields_defaults_and_boundaries(tmp_path):
     p = c.get_params()
     assert (p.fluid_nx, p.fluid_ny, p.fluid_viscosity, p.dt, p.fluid_dx) == (16, 8, 0.02, 0.0025, 0.005)
     assert p.fluid_density == 1000.0 and p.solid_solver_type == "static" and p.output_frequency == 100
-    assert p.boundary_velocities == [0.05, 0.0, 0.0, 0.0]
+    assert p.boundary_velocities == [float(np.float32(0.05)), 0.0, 0.0, 0.0]  # std::vector<float>
     assert [b.flag for b in p.boundaries] == [13, 20, 5, 0]
     s = p.solids[0]
     assert s.mesh_path == "fish.mesh" and s.translate == [1.0, 2.0] and s.rotate == 30.0 and s.density == 50.0
