@@ -49,7 +49,7 @@ struct ffs_lbm {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     // stage timing (ffs_lbm_profile_*)
-    bool profiling = false;
+    int profiling = 0;  // 0 off, 1 stage events, 2 stage events with detection serialised
     struct Mark { int stage; cudaEvent_t a, b; };
     std::vector<Mark> marks;
     std::vector<cudaEvent_t> event_pool;
@@ -220,6 +220,7 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const SurfaceArg
     const bool surf = sa.ne > 0;
     StepScalars sc{h->cl, h->ct, h->cf};
     uint32_t *words = reinterpret_cast<uint32_t *>(h->flags);
+    const bool serial = h->profiling == 2;
     if (DIM == 3 && h->dense_variant < 0) h->dense_variant = tune_dense3d<T>(g, st);
     if (surf) {
         if (h->lt.cap == 0 || (int64_t)h->lt.acc_cap < sa.nv) {
@@ -229,14 +230,20 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const SurfaceArg
         }
         // Link detection and the dense pass overlap: the dense pass skips
         // cells whose LINK bit it sees, but any link cell it does update is
-        // rewritten by link_cells, which runs after both.
-        FFS_CK(cudaEventRecord(h->fork, st));
-        FFS_CK(cudaStreamWaitEvent(h->side, h->fork, 0));
-        {
-            StageTimer t(h, 0, h->side);
-            FFS_CK((launch_detect_links<DIM, T>(g, words, h->lt, sa, sc, h->side)));
+        // rewritten by link_cells, which runs after both.  Serial profiling
+        // runs detection on the caller's stream first, so that each stage's
+        // events time that stage alone (same results: the order only
+        // changes which link cells the dense pass skips).
+        const cudaStream_t ds = serial ? st : h->side;
+        if (!serial) {
+            FFS_CK(cudaEventRecord(h->fork, st));
+            FFS_CK(cudaStreamWaitEvent(h->side, h->fork, 0));
         }
-        FFS_CK(cudaEventRecord(h->join, h->side));
+        {
+            StageTimer t(h, 0, ds);
+            FFS_CK((launch_detect_links<DIM, T>(g, words, h->lt, sa, sc, ds)));
+        }
+        if (!serial) FFS_CK(cudaEventRecord(h->join, h->side));
     }
     {
         StageTimer t(h, 1, st);
@@ -244,7 +251,7 @@ template <int DIM, typename T> ffs_status step_impl(ffs_lbm *h, const SurfaceArg
         else FFS_CK(launch_dense3d<T>(g, st, h->dense_variant));
     }
     if (surf) {
-        FFS_CK(cudaStreamWaitEvent(st, h->join, 0));
+        if (!serial) FFS_CK(cudaStreamWaitEvent(st, h->join, 0));
         const bool fold = (long long)sa.nv * DIM <= kFoldForcesMax;
         {
             StageTimer t(h, 2, st);
@@ -673,7 +680,8 @@ ffs_status ffs_lbm_debug_links(ffs_lbm *h, const ffs_surface *s, uint64_t *cell_
 ffs_status ffs_lbm_profile_enable(ffs_lbm *h, int enable)
 {
     if (!h) return fail(FFS_ERR_INVALID_ARGUMENT, "null grid");
-    h->profiling = enable != 0;
+    if (enable < 0 || enable > 2) return fail(FFS_ERR_INVALID_ARGUMENT, "profile mode must be 0, 1 or 2");
+    h->profiling = enable;
     return FFS_OK;
 }
 

@@ -275,19 +275,35 @@ __device__ __forceinline__ uint32_t vel_dither(size_t idx, float rho)
 // to the magnitude bits of the float and truncating the 13 bits binary16
 // does not keep rounds up with probability (dropped bits) / 2^13, to within
 // 2^-10 of an ulp; values below binary16's normal range (2^-14) or at its
-// top round to nearest.
-__device__ __forceinline__ __half half_sr(float v, uint32_t r)
+// top round to nearest.  `back` receives the value the result represents:
+// in range, the truncated float itself (it has binary16's 11 significant
+// bits, so the conversion is exact), which saves converting back.  The add
+// goes to the whole float: below the top of the range the magnitude cannot
+// carry into the sign bit.
+__device__ __forceinline__ __half half_sr(float v, uint32_t r, float &back)
 {
     const uint32_t b = __float_as_uint(v), mag = b & 0x7fffffffu;
-    if (mag < 0x38800000u || mag >= 0x47000000u) return __float2half_rn(v);
-    return __float2half_rn(__uint_as_float((b & 0x80000000u) | ((mag + (r << 3)) & ~0x1fffu)));
+    if (mag < 0x38800000u || mag >= 0x47000000u) {
+        const __half h = __float2half_rn(v);
+        back = __half2float(h);
+        return h;
+    }
+    back = __uint_as_float((b + (r << 3)) & ~0x1fffu);
+    return __float2half_rn(back);
 }
-template <typename T> __device__ __forceinline__ T to_vel_sr(float v, uint32_t r);
-template <> __device__ __forceinline__ float to_vel_sr<float>(float v, uint32_t) { return v; }
-template <> __device__ __forceinline__ __half to_vel_sr<__half>(float v, uint32_t r) { return half_sr(v, r); }
-template <> __device__ __forceinline__ __nv_bfloat16 to_vel_sr<__nv_bfloat16>(float v, uint32_t r)
+template <typename T> __device__ __forceinline__ T to_vel_sr(float v, uint32_t r, float &back);
+template <> __device__ __forceinline__ float to_vel_sr<float>(float v, uint32_t, float &back)
 {
-    return __ushort_as_bfloat16(__half_as_ushort(half_sr(v, r)));
+    back = v;
+    return v;
+}
+template <> __device__ __forceinline__ __half to_vel_sr<__half>(float v, uint32_t r, float &back)
+{
+    return half_sr(v, r, back);
+}
+template <> __device__ __forceinline__ __nv_bfloat16 to_vel_sr<__nv_bfloat16>(float v, uint32_t r, float &back)
+{
+    return __ushort_as_bfloat16(__half_as_ushort(half_sr(v, r, back)));
 }
 
 // The stored form of moment vector m of cell idx: FP32 as is; reduced
@@ -307,13 +323,13 @@ __device__ __forceinline__ void encode_values(const float *m, size_t idx, const 
         const uint32_t h = vel_dither(idx, m[0]);
 #pragma unroll
         for (int a = 0; a < DIM; ++a) {
-            const T s = to_vel_sr<T>(m[1 + a] * c.su, (h >> (10 * a)) & 0x3ffu);
-            enc[1 + a] = s;
-            ud[a] = StorageTraits<T>::from_vel(s) * c.inv_su;
+            float back;
+            enc[1 + a] = to_vel_sr<T>(m[1 + a] * c.su, (h >> (10 * a)) & 0x3ffu, back);
+            ud[a] = back * c.inv_su;
         }
 #pragma unroll
         for (int k = DIM + 1; k < NM; ++k)
-            enc[k] = StorageTraits<T>::to((m[k] - ud[MomentLayout<DIM>::pa(k)] * ud[MomentLayout<DIM>::pb(k)]) * c.sp);
+            enc[k] = StorageTraits<T>::to(fmaf(-ud[MomentLayout<DIM>::pa(k)], ud[MomentLayout<DIM>::pb(k)], m[k]) * c.sp);
     }
 }
 

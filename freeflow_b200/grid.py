@@ -254,9 +254,12 @@ class FluidGrid:
         A.check(A.load().ffs_lbm_get_status(self._h, C.byref(v), int(clear), _stream_handle(stream)), "get_status")
         return int(v.value)
 
-    def profile(self, enable: bool = True):
-        """Start/stop per-stage CUDA-event timing of the steps."""
-        A.check(A.load().ffs_lbm_profile_enable(self._h, int(bool(enable))), "profile_enable")
+    def profile(self, enable: bool = True, serial: bool = False):
+        """Start/stop per-stage CUDA-event timing of the steps.  serial=True
+        moves link detection off its side stream, ahead of the dense pass, so
+        that each stage is timed alone (the step loses the overlap)."""
+        mode = (2 if serial else 1) if enable else 0
+        A.check(A.load().ffs_lbm_profile_enable(self._h, mode), "profile_enable")
 
     def profile_read(self, reset: bool = True) -> dict:
         """{stage: (milliseconds, launches)} summed since the last reset."""

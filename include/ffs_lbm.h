@@ -256,7 +256,11 @@ ffs_status ffs_lbm_debug_links(ffs_lbm *grid, const ffs_surface *surface, uint64
  * the summed milliseconds and launch counts per stage:
  * [0] link detection, [1] dense fused update, [2] link cells, [3] forces.
  * For surfaces of at most 2048 force components the force conversion runs in
- * the last CTA of the link-cell kernel, and [3] records no launch. */
+ * the last CTA of the link-cell kernel, and [3] records no launch.
+ * enable: 0 off; 1 on; 2 on with link detection moved from its side stream
+ * onto the step's stream ahead of the dense pass, so that every stage is
+ * timed alone (a measurement mode: the step is then slower by the overlap it
+ * gives up; results are the same). */
 typedef struct {
     double ms[4];
     int64_t launches[4];
