@@ -132,6 +132,186 @@ __device__ __forceinline__ void slice_init_plus(float *R, const float *Y)
     R[3] = Y[0]; R[6] = Y[0]; R[8] = Y[1]; R[9] = Y[3];
 }
 
+// Paired layout (variant 2).  For each (c_x, c_y) set and halo cell,
+// the c_z = -1 and +1 populations sit side by side as one float2 (a plane of
+// 9 x kHalo float2), and the c_z = 0 population in a plane of floats after
+// it: the cells of a tile pull the three from the same neighbour, so one
+// 64-bit and one 32-bit load replace three, the reconstruction stores them
+// the same way, and the c_z = -1 / +1 pair is one 64-bit register pair for
+// the packed f32x2 arithmetic below.  The plane has the size of the scalar
+// layout's.  Per element, every operation is the scalar layout's, in the
+// same order: all variants give identical bits.
+constexpr int kPairFloats = 9 * kHalo * 2;  // the float2 plane; the c_z = 0 plane follows
+// float index of population (kx, ky, kz) (k = c + 1) of halo cell c
+template <bool PAIRED> __device__ __forceinline__ int pop_index(int kx, int ky, int kz, int c)
+{
+    if constexpr (PAIRED) {
+        const int s9 = (kx + 3 * ky) * kHalo + c;
+        return kz == 1 ? kPairFloats + s9 : 2 * s9 + (kz == 2);
+    } else {
+        return set_of(kx, ky, kz) * kHalo + c;
+    }
+}
+__device__ __forceinline__ void store_pair(float *buf, int s9, f2 p, float mid)
+{
+    *reinterpret_cast<unsigned long long *>(buf + 2 * s9) = p.v;
+    buf[kPairFloats + s9] = mid;
+}
+__device__ __forceinline__ void load_pair(const float *buf, int s9, float &lo, float &hi, float &mid)
+{
+    const float2 v = *reinterpret_cast<const float2 *>(buf + 2 * s9);
+    lo = v.x;
+    hi = v.y;
+    mid = buf[kPairFloats + s9];
+}
+
+// slice_sums of the c_z = -1 and +1 slices (as the lo and hi halves of Sp)
+// and of the c_z = 0 slice (Sm), from the paired layout
+__device__ __forceinline__ void slice_sums_paired(const float *buf, int c_own, f2 *Sp, float *Sm)
+{
+    const f2 quarter = f2splat(0.25f);
+    f2 X0p[3], X1p[3], X2p[3];
+    float X0m[3], X1m[3], X2m[3];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky) {
+        const int crow = c_own - (ky - 1) * kHX;
+        float4 a, b, d;   // x, y: c_z = -1, +1; z: c_z = 0
+        load_pair(buf, (3 * ky) * kHalo + crow + 1, a.x, a.y, a.z);
+        load_pair(buf, (1 + 3 * ky) * kHalo + crow, b.x, b.y, b.z);
+        load_pair(buf, (2 + 3 * ky) * kHalo + crow - 1, d.x, d.y, d.z);
+        const f2 fm = f2make(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f));
+        const f2 f0 = f2make(fmaxf(b.x, 0.0f), fmaxf(b.y, 0.0f));
+        const f2 fp = f2make(fmaxf(d.x, 0.0f), fmaxf(d.y, 0.0f));
+        const f2 sp = fp + fm;
+        X1p[ky] = fp - fm;
+        X0p[ky] = vfma(quarter, sp, f0);
+        X2p[ky] = sp;
+        const float gm = fmaxf(a.z, 0.0f), g0 = fmaxf(b.z, 0.0f), gp = fmaxf(d.z, 0.0f);
+        const float sm = gp + gm;
+        X1m[ky] = gp - gm;
+        X0m[ky] = fmaf(0.25f, sm, g0);
+        X2m[ky] = sm;
+    }
+    const f2 s0 = X0p[2] + X0p[0];
+    Sp[0] = vfma(quarter, s0, X0p[1]);
+    Sp[1] = X0p[2] - X0p[0];
+    Sp[2] = s0;
+    Sp[3] = vfma(quarter, X1p[2] + X1p[0], X1p[1]);
+    Sp[4] = X1p[2] - X1p[0];
+    Sp[5] = vfma(quarter, X2p[2] + X2p[0], X2p[1]);
+    const float t0 = X0m[2] + X0m[0];
+    Sm[0] = fmaf(0.25f, t0, X0m[1]);
+    Sm[1] = X0m[2] - X0m[0];
+    Sm[2] = t0;
+    Sm[3] = fmaf(0.25f, X1m[2] + X1m[0], X1m[1]);
+    Sm[4] = X1m[2] - X1m[0];
+    Sm[5] = fmaf(0.25f, X2m[2] + X2m[0], X2m[1]);
+}
+
+// The z level of Coef3V::populations_each (the Hermite sums over c_z of the
+// six coefficient groups), with the c_z = -1 / +1 entries as pairs (p) and
+// the c_z = 0 entry apart (m): herm3v gives ((a0 + a2) - a1, fma(-1/2, a2,
+// a0), (a0 + a2) + a1), herm2v (a0 - a1, a0, a0 + a1).
+struct ZLevel {
+    f2 p00, p10, p01, p20, p02, p11;
+    float m00, m10, m01, m20, m02, m11;
+    __device__ __forceinline__ explicit ZLevel(const Coef3V<float> &c)
+    {
+        auto h3 = [](float a0, float a1, float a2, f2 &p, float &m) {
+            const float t = a0 + a2;
+            p = f2make(t - a1, t + a1);
+            m = fmaf(-0.5f, a2, a0);
+        };
+        auto h2 = [](float a0, float a1, f2 &p, float &m) {
+            p = f2make(a0 - a1, a0 + a1);
+            m = a0;
+        };
+        h3(c.rho, c.m1z, c.m2zz, p00, m00);
+        h3(c.m1x, c.m2xz, c.qxzz, p10, m10);
+        h3(c.m1y, c.m2yz, c.qyzz, p01, m01);
+        h2(c.m2xx, c.qxxz, p20, m20);
+        h2(c.m2yy, c.qyyz, p02, m02);
+        h2(c.m2xy, c.qxyz, p11, m11);
+    }
+};
+
+// All 27 unweighted populations of one cell into the paired layout: the y and
+// x levels of populations_each, paired over c_z = -1 / +1.
+__device__ __forceinline__ void store_populations_paired(const Coef3V<float> &c, float *buf, int cell)
+{
+    const ZLevel z(c);
+    f2 C0p[3], C1p[3], C2p[3];
+    float C0m[3], C1m[3], C2m[3];
+    herm3v(z.p00, z.p01, z.p02, C0p);
+    herm3v(z.p10, z.p11, f2splat(c.qxyy), C1p);
+    herm2v(z.p20, f2splat(c.qxxy), C2p);
+    herm3v(z.m00, z.m01, z.m02, C0m);
+    herm3v(z.m10, z.m11, c.qxyy, C1m);
+    herm2v(z.m20, c.qxxy, C2m);
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky) {
+        f2 Fp[3];
+        float Fm[3];
+        herm3v(C0p[ky], C1p[ky], C2p[ky], Fp);
+        herm3v(C0m[ky], C1m[ky], C2m[ky], Fm);
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) store_pair(buf, (kx + 3 * ky) * kHalo + cell, Fp[kx], Fm[kx]);
+    }
+}
+
+// The 9 populations with c_y = KY - 1 of a halo row cell (populations_row)
+// into the paired layout.
+template <int KY> __device__ __forceinline__ void store_row_paired(const Coef3V<float> &c, float *buf, int cell)
+{
+    const ZLevel z(c);
+    auto h3p = [](f2 a0, f2 a1, f2 a2) {
+        if constexpr (KY == 1) return vfma(f2splat(-0.5f), a2, a0);
+        else if constexpr (KY == 0) return (a0 + a2) - a1;
+        else return (a0 + a2) + a1;
+    };
+    auto h2p = [](f2 a0, f2 a1) {
+        if constexpr (KY == 1) return a0;
+        else if constexpr (KY == 0) return a0 - a1;
+        else return a0 + a1;
+    };
+    auto h3m = [](float a0, float a1, float a2) {
+        if constexpr (KY == 1) return fmaf(-0.5f, a2, a0);
+        else if constexpr (KY == 0) return (a0 + a2) - a1;
+        else return (a0 + a2) + a1;
+    };
+    auto h2m = [](float a0, float a1) {
+        if constexpr (KY == 1) return a0;
+        else if constexpr (KY == 0) return a0 - a1;
+        else return a0 + a1;
+    };
+    f2 Fp[3];
+    float Fm[3];
+    herm3v(h3p(z.p00, z.p01, z.p02), h3p(z.p10, z.p11, f2splat(c.qxyy)), h2p(z.p20, f2splat(c.qxxy)), Fp);
+    herm3v(h3m(z.m00, z.m01, z.m02), h3m(z.m10, z.m11, c.qxyy), h2m(z.m20, c.qxxy), Fm);
+#pragma unroll
+    for (int kx = 0; kx < 3; ++kx) store_pair(buf, (kx + 3 * KY) * kHalo + cell, Fp[kx], Fm[kx]);
+}
+
+// The 9 populations with c_x = sx of a halo column cell (populations_col)
+// into the paired layout; kx = sx + 1.
+__device__ __forceinline__ void store_col_paired(const Coef3V<float> &c, float sx, int kx, float *buf, int cell)
+{
+    const ZLevel z(c);
+    f2 C0p[3], C1p[3], C2p[3];
+    float C0m[3], C1m[3], C2m[3];
+    herm3v(z.p00, z.p01, z.p02, C0p);
+    herm3v(z.p10, z.p11, f2splat(c.qxyy), C1p);
+    herm2v(z.p20, f2splat(c.qxxy), C2p);
+    herm3v(z.m00, z.m01, z.m02, C0m);
+    herm3v(z.m10, z.m11, c.qxyy, C1m);
+    herm2v(z.m20, c.qxxy, C2m);
+    const f2 sxp = f2splat(sx);
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+        store_pair(buf, (kx + 3 * ky) * kHalo + cell, vfma(sxp, C1p[ky], C0p[ky] + C2p[ky]),
+                   fmaf(sx, C1m[ky], C0m[ky] + C2m[ky]));
+}
+
 // R'' += (basis(c) w F) / (W0 s) for one unweighted population F of
 // direction c: the weight and the scales are powers of two
 __device__ __forceinline__ void add_basis_scaled(float *R, int cx, int cy, int cz, float F)
@@ -174,6 +354,7 @@ __device__ __forceinline__ void add_basis_rt(float *R, int cx, int cy, int cz, f
 // R'' += basis(c_i) w_i max(0, F_inv(i)(x)) (scaled as above) for every wall
 // direction i in w, with the cell's own unweighted populations read from the
 // current plane.
+template <bool PAIRED>
 __device__ __forceinline__ void add_reflected(const float *buf, int c_own, uint32_t w, float (&R)[10])
 {
 #pragma unroll
@@ -184,7 +365,7 @@ __device__ __forceinline__ void add_reflected(const float *buf, int c_own, uint3
             for (int kx = 0; kx < 3; ++kx) {
                 const int i = dir_index<3>(kx, ky, kz);
                 if (i == 0) continue;
-                float f = fmaxf(buf[set_of(2 - kx, 2 - ky, 2 - kz) * kHalo + c_own], 0.0f);
+                float f = fmaxf(buf[pop_index<PAIRED>(2 - kx, 2 - ky, 2 - kz, c_own)], 0.0f);
                 f = (w & (1u << i)) ? f : 0.0f;
                 add_basis_scaled(R, kx - 1, ky - 1, kz - 1, f);
             }
@@ -195,6 +376,7 @@ __device__ __forceinline__ void add_reflected(const float *buf, int c_own, uint3
 // face the halo cell holds real populations, but the wrapped test found a
 // wall, so the step takes the cell's reflected population instead
 // (add_reflected).
+template <bool PAIRED>
 __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint32_t w, int kz_sel, float (&R)[10])
 {
     while (w) {
@@ -203,7 +385,7 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
         int cx, cy, cz;
         dir_vec<3>(i, cx, cy, cz);
         if (cz + 1 == kz_sel) {
-            const float pulled = fmaxf(buf[set_of(cx + 1, cy + 1, cz + 1) * kHalo + c_own - cx - cy * kHX], 0.0f);
+            const float pulled = fmaxf(buf[pop_index<PAIRED>(cx + 1, cy + 1, cz + 1, c_own - cx - cy * kHX)], 0.0f);
             add_basis_scaled(R, cx, cy, cz, -pulled);
         }
     }
@@ -216,10 +398,13 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
 // bits, as it does for grids of up to 429 M cells; each access then takes one
 // 32-bit index and one widening multiply-add instead of 64-bit arithmetic,
 // which saves registers (112 against 122) and about 5 % of the pass.
-template <typename T, int MINB, bool IDX32>
+// PAIRED: the paired shared-memory layout with packed c_z = -1 / +1
+// arithmetic (variant 2); otherwise one float plane per population
+// (variants 0 and 1).
+template <typename T, int MINB, bool IDX32, bool PAIRED>
 __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T> g, int zchunk)
 {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
     const int zb = blockIdx.z * zchunk;
@@ -305,8 +490,13 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     };
     auto recon_cell = [&](float *buf, const T *raw, bool zero, int c) {
         if (zero) {
+            if constexpr (PAIRED) {
 #pragma unroll
-            for (int j = 0; j < 27; ++j) buf[j * kHalo + c] = 0.0f;
+                for (int j = 0; j < 9; ++j) store_pair(buf, j * kHalo + c, f2make(0.0f, 0.0f), 0.0f);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 27; ++j) buf[j * kHalo + c] = 0.0f;
+            }
             return;
         }
         float m[10];
@@ -315,7 +505,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         decode_moments<3, T>(m, g.codec);
         Coef3V<float> cf;
         cf.make(m);
-        cf.populations_each<false>([&](int kz, int ky, int kx, float v) { buf[set_of(kx, ky, kz) * kHalo + c] = v; });
+        if constexpr (PAIRED) store_populations_paired(cf, buf, c);
+        else cf.populations_each<false>([&](int kz, int ky, int kx, float v) { buf[set_of(kx, ky, kz) * kHalo + c] = v; });
     };
     // A ring cell feeds the tile only the 9 populations that point into it:
     // c_y = +1 from the row below (warp 0), c_y = -1 from the row above
@@ -324,10 +515,21 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     // ever read.
     const int ring_kind = tid < 32 ? 0 : tid < 64 ? 1 : 2;
     const float ring_sx = tid < 74 ? 1.0f : -1.0f;                 // columns: c_x of the fed populations
-    const int ring_kxo = (tid < 74 ? 2 : 0) * kHalo;               // their kx plane offset
+    const int ring_kx = tid < 74 ? 2 : 0;                          // their kx = c_x + 1
+    const int ring_kxo = ring_kx * kHalo;                          // and its plane offset
     auto recon_ring = [&](float *buf, bool zero) {
         const int c = c_ring;
         if (zero) {
+            if constexpr (PAIRED) {
+                const f2 z2 = f2make(0.0f, 0.0f);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (ring_kind == 0) store_pair(buf, (k + 6) * kHalo + c, z2, 0.0f);
+                    else if (ring_kind == 1) store_pair(buf, k * kHalo + c, z2, 0.0f);
+                    else store_pair(buf, (ring_kx + 3 * k) * kHalo + c, z2, 0.0f);
+                }
+                return;
+            }
 #pragma unroll
             for (int kz = 0; kz < 3; ++kz)
 #pragma unroll
@@ -344,6 +546,12 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         decode_moments<3, T>(m, g.codec);
         Coef3V<float> cf;
         cf.make(m);
+        if constexpr (PAIRED) {
+            if (ring_kind == 0) store_row_paired<2>(cf, buf, c);
+            else if (ring_kind == 1) store_row_paired<0>(cf, buf, c);
+            else store_col_paired(cf, ring_sx, ring_kx, buf, c);
+            return;
+        }
         if (ring_kind == 0)
             cf.populations_row<2>([&](int kz, int kx, float v) { buf[set_of(kx, 2, kz) * kHalo + c] = v; });
         else if (ring_kind == 1)
@@ -385,39 +593,64 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         const uint32_t wn = (upd_n && (fn & (kBitNearWall | kBitOutletSrc))) ? g.wallmask[cell_at(p + 1)] : 0u;
         __syncthreads();
         if (inside) {
-            float S[6];
-            slice_sums(buf, 0, c_own, S);
-            slice_add<-1>(Rp, S);
-            slice_sums(buf, 1, c_own, S);
-            slice_add<0>(Rc, S);
             constexpr uint32_t kWall = wall_bits_mask<3>();
-            if (wc & kWall) add_reflected(buf, c_own, wc & kWall, Rc);
+            // the cell at z = p - 1 is complete: collide, store, feed outlets
+            auto finish = [&](const float (&R)[10]) {
+                const int d = p - 1;
+                if (d >= zb && is_updated(fp & kTypeMask) && !(fp & kBitLink)) {
+                    const uint32_t idx = (uint32_t)(d * nxy + col);
+                    float m[10];
+                    collide3(R, g.omega, m);
+                    if constexpr (IDX32) encode_store_idx32<3, T>(m, g.dst, idx, g.ncell, g.codec);
+                    else encode_store_strided<3, T>(m, g.dst, (size_t)idx, g.ncell, g.codec);
+                    if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
+                    if (fp & kBitOutletSrc) {
+                        float ms[10];
+                        stored_values<3, T>(m, ms, idx, g.codec);
+                        feed_outlets<3, T>(g, idx, ms, wp);
+                    }
+                }
+            };
             // wall directions across a high face (their halo cell held real
             // populations): remove the pulled value, per destination cell
             // z = p-1 (c_z = -1 slice) and z = p (c_z = 0)
             const uint32_t oor_p = oor_xy | ((p - 1 == g.nz - 1) ? oor_zhi : 0u);
-            if (wp & kWall & oor_p) wall_fix_part(buf, c_own, wp & kWall & oor_p, 0, Rp);
-            if (wc & kWall & oor_xy) wall_fix_part(buf, c_own, wc & kWall & oor_xy, 1, Rc);
-            // the cell at z = p - 1 is complete
-            const int d = p - 1;
-            if (d >= zb && is_updated(fp & kTypeMask) && !(fp & kBitLink)) {
-                const uint32_t idx = (uint32_t)(d * nxy + col);
-                float R[10], m[10];
+            if constexpr (PAIRED) {
+                f2 Sp[6];
+                float Sm[6], lo[6], hi[6];
+                slice_sums_paired(buf, c_own, Sp, Sm);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) f2split(Sp[k], lo[k], hi[k]);
+                slice_add<-1>(Rp, lo);
+                slice_add<0>(Rc, Sm);
+                if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
+                if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
+                if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                float R[10];
                 raw_from_scaled(Rp, R);
-                collide3(R, g.omega, m);
-                if constexpr (IDX32) encode_store_idx32<3, T>(m, g.dst, idx, g.ncell, g.codec);
-                else encode_store_strided<3, T>(m, g.dst, (size_t)idx, g.ncell, g.codec);
-                if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
-                if (fp & kBitOutletSrc) {
-                    float ms[10];
-                    stored_values<3, T>(m, ms, idx, g.codec);
-                    feed_outlets<3, T>(g, idx, ms, wp);
+                // Rp is free: it becomes the cell at z = p + 1
+                slice_init_plus(Rp, hi);
+                if (wn & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wn & kWall & oor_xy, 2, Rp);
+                finish(R);
+            } else {
+                float S[6];
+                slice_sums(buf, 0, c_own, S);
+                slice_add<-1>(Rp, S);
+                slice_sums(buf, 1, c_own, S);
+                slice_add<0>(Rc, S);
+                if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
+                if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
+                if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                {
+                    float R[10];
+                    raw_from_scaled(Rp, R);
+                    finish(R);
                 }
+                // Rp is free: it becomes the cell at z = p + 1
+                slice_sums(buf, 2, c_own, S);
+                slice_init_plus(Rp, S);
+                if (wn & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wn & kWall & oor_xy, 2, Rp);
             }
-            // Rp is free: it becomes the cell at z = p + 1
-            slice_sums(buf, 2, c_own, S);
-            slice_init_plus(Rp, S);
-            if (wn & kWall & oor_xy) wall_fix_part(buf, c_own, wn & kWall & oor_xy, 2, Rp);
         }
         fp = fc; fc = fn; fn = fnn;
         wp = wc; wc = wn;
@@ -480,31 +713,32 @@ static int choose_zchunks(int tiles, int nz, int slots)
     return best;
 }
 
-template <typename T, int MINB, bool IDX32> struct Dense3dLaunchAs {
+template <typename T, int MINB, bool IDX32, bool PAIRED> struct Dense3dLaunchAs {
     static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
     {
         int slots = 0;
-        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_kernel<T, MINB, IDX32>), D3::kThreads,
-                                       D3::kSmemBytes, slots);
+        constexpr size_t smem = D3::kSmemBytes;
+        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_kernel<T, MINB, IDX32, PAIRED>),
+                                       D3::kThreads, smem, slots);
         if (e != cudaSuccess) return e;
         int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY;
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
         dim3 grid(tx, ty, (g.nz + zchunk - 1) / zchunk);
-        dense3d_kernel<T, MINB, IDX32><<<grid, D3::kThreads, D3::kSmemBytes, s>>>(g, zchunk);
+        dense3d_kernel<T, MINB, IDX32, PAIRED><<<grid, D3::kThreads, smem, s>>>(g, zchunk);
         return cudaGetLastError();
     }
 };
 
 // 32-bit indices whenever every moment index of the grid fits (FFS_DENSE3D_INDEX64
 // forces 64-bit indices, so that tests reach that path on small grids)
-template <typename T, int MINB> struct Dense3dLaunch {
+template <typename T, int MINB, bool PAIRED> struct Dense3dLaunch {
     static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
     {
         const char *force64 = std::getenv("FFS_DENSE3D_INDEX64");
         if (10ull * g.ncell <= 0xFFFFFFFFull && !(force64 && force64[0] == '1'))
-            return Dense3dLaunchAs<T, MINB, true>::run(g, s);
-        return Dense3dLaunchAs<T, MINB, false>::run(g, s);
+            return Dense3dLaunchAs<T, MINB, true, PAIRED>::run(g, s);
+        return Dense3dLaunchAs<T, MINB, false, PAIRED>::run(g, s);
     }
 };
 
@@ -514,7 +748,11 @@ template <typename T> bool dense3d_has_variant(int v) { return v >= 0 && v < kDe
 template <typename T>
 cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
 {
-    return variant == 1 ? Dense3dLaunch<T, 3>::run(g, s) : Dense3dLaunch<T, 2>::run(g, s);
+    switch (variant) {
+    case 1: return Dense3dLaunch<T, 3, false>::run(g, s);
+    case 2: return Dense3dLaunch<T, 2, true>::run(g, s);
+    default: return Dense3dLaunch<T, 2, false>::run(g, s);
+    }
 }
 
 // Times each variant on this grid (the pass only reads src and writes dst, so
@@ -532,8 +770,8 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     cudaEventCreate(&b);
     float best = 1e30f;
     int best_v = 0;
-    // the single-plane kernel for two and three CTAs per SM, which round
-    // identically
+    // the scalar layout for two and three CTAs per SM and the paired layout,
+    // which all round identically
     for (int v = 0; v < kDense3dVariants; ++v) {
         if (!dense3d_has_variant<T>(v)) continue;
         if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue; // warm-up

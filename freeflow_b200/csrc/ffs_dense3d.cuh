@@ -13,10 +13,12 @@ struct D3 {
 };
 static_assert(D3::kRing <= D3::kThreads, "every ring cell needs a partner thread");
 
-// variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM.  Both
-// round identically; the first step times them and keeps the faster
+// variant: 0 = two CTAs per SM (no spills), 1 = three CTAs per SM, 2 = two
+// CTAs per SM with the paired shared-memory layout and packed c_z = -1 / +1
+// arithmetic (a three-CTA build of it spills and ran 40 % slower).  All
+// round identically; the first step times them and keeps the fastest
 // (FFS_DENSE3D_VARIANT pins one).
-constexpr int kDense3dVariants = 2;
+constexpr int kDense3dVariants = 3;
 template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant);
 template <typename T> int tune_dense3d(const GridArgs<T> &g, cudaStream_t s);
 

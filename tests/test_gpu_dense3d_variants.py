@@ -2,7 +2,8 @@
 per grid by speed, so each must pass the parity cases on its own).
 
 Variants: 0 and 1 are the single-plane z-march built for two and three CTAs
-per SM.
+per SM; 2 is the two-CTA march with the paired shared-memory layout and
+packed c_z = -1 / +1 arithmetic.
 Tolerances are those of test_gpu_parity.py: 2e-6 against the ref32 oracle,
 4e-6 next to walls (bounce-back added as a correction), 5e-6 against FP64.
 """
@@ -18,7 +19,7 @@ pytestmark = pytest.mark.gpu
 # (variant, index width): the single-plane variants run with 32-bit indices on
 # grids of up to 429 M cells and 64-bit ones beyond; FFS_DENSE3D_INDEX64 forces
 # the 64-bit path here
-VARIANTS = [(0, 32), (1, 32), (0, 64), (1, 64)]
+VARIANTS = [(0, 32), (1, 32), (2, 32), (0, 64), (1, 64), (2, 64)]
 
 
 @pytest.fixture(params=VARIANTS, ids=lambda v: f"v{v[0]}-i{v[1]}")
@@ -105,8 +106,8 @@ def test_odd_width(cuda, variant):
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 def test_tuned_variants_round_identically(cuda, monkeypatch, storage):
-    """The first step's timing chooses between variants 0 and 1, so both must
-    give the same bits (moments and surface forces, with walls, an inlet, an
+    """The first step's timing chooses among the variants, so all must give
+    the same bits (moments and surface forces, with walls, an inlet, an
     outlet and a moving surface): the choice cannot change a result."""
     import torch
 
@@ -114,7 +115,7 @@ def test_tuned_variants_round_identically(cuda, monkeypatch, storage):
 
     wl = W.swimmer_3d(nx=64, ny=32, nz=32, body_frac=0.4, nlat=16, nlon=24, seed=4)
     out = []
-    for v in ("0", "1"):
+    for v in ("0", "1", "2"):
         monkeypatch.setenv("FFS_DENSE3D_VARIANT", v)
         g, s = make_gpu(wl, storage)
         for k in range(6):
@@ -124,5 +125,6 @@ def test_tuned_variants_round_identically(cuda, monkeypatch, storage):
         assert g.status() == 0
         out.append((g.get_moments(), s.forces64.cpu().numpy()))
         g.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        assert np.array_equal(out[0][1], o[1])
