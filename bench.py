@@ -383,13 +383,16 @@ def run_reference(args):
 
 # ---------------------------------------------------------------- serving
 def run_serving(iterations: int, warmup: int, concurrencies=(64, 256, 512), plain_steps: int = 20,
-                plain_seconds: float = 1.0, seed: int = 0):
+                plain_seconds: float = 1.0, seed: int = 0, pipelined_at=(256,)):
     """Config E: Poisson stream of 2D swimmer episodes (grids uniform over
     256x128, 512x192, 1200x400; 8 actions per control step; 10 substeps per
     action; lengths uniform in 200..2000 control steps) through the FP16 pool
     with continuous batching, at each mean concurrency, against the plain
     per-episode FP32 path (one episode of each grid size at a time, at least
-    `plain_seconds` of control steps each)."""
+    `plain_seconds` of control steps each).  At the concurrencies in
+    `pipelined_at` the same stream also runs through serve_pipelined (two
+    pools stepping in turn); its iterations each serve one of the two groups,
+    so it runs twice the iterations for the same number of control steps."""
     import torch
     from freeflow_b200 import serving as S
 
@@ -411,8 +414,22 @@ def run_serving(iterations: int, warmup: int, concurrencies=(64, 256, 512), plai
         pool.close()
         torch.cuda.synchronize()
         dense_gbs = info["tuned_cells"] * 25 / (info["dense_ms"] * 1e-3) / 1e9 if info["dense_ms"] > 0 else None
+        piped = None
+        if concurrency in pipelined_at:
+            # the same request stream over two pools stepping in turn: host
+            # work on one group overlaps the GPU step of the other
+            pools = [S.Pool(storage="f16", budget_bytes=3 << 30, max_episodes=min(1000, concurrency), substeps=10,
+                            num_actions=8) for _ in range(2)]
+            rp = S.serve_pipelined(pools, specs, iterations=2 * iterations, initial=concurrency,
+                                   arrivals_per_iter=per_iter, seed=seed, warmup_iterations=2 * warmup)
+            for pl in pools:
+                pl.close()
+            torch.cuda.synchronize()
+            piped = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in rp.items()}
+            piped["speedup_vs_plain"] = round(rp["env_steps_per_s"] / plain["env_steps_per_s"], 2)
         by_c[str(concurrency)] = {
             "batched": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()},
+            "pipelined_two_pools": piped,
             "speedup_vs_plain": round(r["env_steps_per_s"] / plain["env_steps_per_s"], 2),
             "pool": {"tile": f"{info['tile_x']}x{info['tile_y']}" + (" strip" if info["strip"] else ""),
                      "graph_builds": info["graph_builds"], "max_episodes": max_episodes,

@@ -25,8 +25,12 @@
 //
 // Ordering: every device operation of a pool is issued on the pool's stream,
 // so an evicted episode's block is reused only after the work that read it.
-// The pinned host buffers are rewritten only after the previous control step
-// has completed (ffs_pool_advance waits for it).
+// The pinned parameter and output buffers are double-buffered: control step
+// k uses buffer k & 1, so ffs_pool_advance waits only for step k - 2 (the
+// last user of the buffer it refills), not for step k - 1, and a caller can
+// enqueue the next control step while the previous one runs.  The pinned
+// active table is refilled only after its last upload has completed (its own
+// event).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -181,9 +185,9 @@ struct ffs_pool {
     std::vector<Slot> slots;
     std::vector<int> order; // admitted slots, admission order
     PoolEpisode *d_eps = nullptr;
-    PoolParams *d_prm = nullptr, *h_prm = nullptr;
+    PoolParams *d_prm = nullptr, *h_prm[2] = {};
     PoolActive *d_act = nullptr, *h_act = nullptr;
-    PoolOutput *d_out = nullptr, *h_out = nullptr;
+    PoolOutput *d_out = nullptr, *h_out[2] = {};
     LinkTable lt;
     uint32_t *owner = nullptr;
     int shape = 1;
@@ -192,8 +196,13 @@ struct ffs_pool {
     double tuned_ms = 0.0;   // one dense pass of the chosen shape at that tuning
     int parity = 0;
     cudaGraphExec_t graph[kPoolNumShapes][2] = {};
-    cudaEvent_t done = nullptr, ev0 = nullptr, ev1 = nullptr;
-    bool inflight = false;
+    // done[b]: the last control step that used pinned buffer b has finished
+    // (its outputs are in h_out[b]); act_sent: the last active-table upload
+    // has read h_act
+    cudaEvent_t done[2] = {}, act_sent = nullptr, ev0 = nullptr, ev1 = nullptr;
+    bool inflight[2] = {false, false};
+    bool act_pending = false;
+    int last = 0;             // buffer of the latest control step
     int64_t advances = 0, graph_builds = 0;
     int sms = 0;              // SMs of the device, queried at creation
     int grid_dense[kPoolNumShapes] = {};
@@ -231,19 +240,35 @@ void build_active(ffs_pool *p)
 
 ffs_status upload_active(ffs_pool *p)
 {
+    if (p->act_pending) {
+        POOL_CK(cudaEventSynchronize(p->act_sent));
+        p->act_pending = false;
+    }
     build_active(p);
     POOL_CK(cudaMemcpyAsync(p->d_act, p->h_act, sizeof(PoolActive), cudaMemcpyHostToDevice, p->st));
+    POOL_CK(cudaEventRecord(p->act_sent, p->st));
+    p->act_pending = true;
     p->act_dirty = false;
     return FFS_OK;
 }
 
-ffs_status wait_idle(ffs_pool *p)
+// Waits for control step(s) in flight on pinned buffer b.
+ffs_status wait_buffer(ffs_pool *p, int b)
 {
-    if (p->inflight) {
-        POOL_CK(cudaEventSynchronize(p->done));
-        p->inflight = false;
+    if (p->inflight[b]) {
+        POOL_CK(cudaEventSynchronize(p->done[b]));
+        p->inflight[b] = false;
     }
     return FFS_OK;
+}
+
+// Waits for every control step in flight (the latest one finishes last: one
+// stream).
+ffs_status wait_idle(ffs_pool *p)
+{
+    ffs_status r = wait_buffer(p, p->last);
+    if (r != FFS_OK) return r;
+    return wait_buffer(p, p->last ^ 1);
 }
 
 template <typename T> ffs_status capture(ffs_pool *p, int shape, int parity, cudaGraphExec_t *out)
@@ -407,13 +432,17 @@ ffs_status ffs_pool_create(const ffs_pool_desc *desc, ffs_pool **out)
     p->arena.reset(p->arena_mem, (size_t)d.budget_bytes);
     if ((e = cudaMalloc(&p->d_eps, sizeof(PoolEpisode) * d.max_episodes)) != cudaSuccess) return bail(e, "episodes");
     if ((e = cudaMalloc(&p->d_prm, sizeof(PoolParams) * d.max_episodes)) != cudaSuccess) return bail(e, "params");
-    if ((e = cudaMallocHost(&p->h_prm, sizeof(PoolParams) * d.max_episodes)) != cudaSuccess) return bail(e, "params");
+    for (int b = 0; b < 2; ++b)
+        if ((e = cudaMallocHost(&p->h_prm[b], sizeof(PoolParams) * d.max_episodes)) != cudaSuccess) return bail(e, "params");
     if ((e = cudaMalloc(&p->d_act, sizeof(PoolActive))) != cudaSuccess) return bail(e, "active table");
     if ((e = cudaMallocHost(&p->h_act, sizeof(PoolActive))) != cudaSuccess) return bail(e, "active table");
     if ((e = cudaMalloc(&p->d_out, sizeof(PoolOutput) * d.max_episodes)) != cudaSuccess) return bail(e, "outputs");
-    if ((e = cudaMallocHost(&p->h_out, sizeof(PoolOutput) * d.max_episodes)) != cudaSuccess) return bail(e, "outputs");
+    for (int b = 0; b < 2; ++b) {
+        if ((e = cudaMallocHost(&p->h_out[b], sizeof(PoolOutput) * d.max_episodes)) != cudaSuccess)
+            return bail(e, "outputs");
+        std::memset(p->h_out[b], 0, sizeof(PoolOutput) * d.max_episodes);
+    }
     std::memset(p->h_act, 0, sizeof(PoolActive));
-    std::memset(p->h_out, 0, sizeof(PoolOutput) * d.max_episodes);
     if ((e = cudaMemset(p->d_act, 0, sizeof(PoolActive))) != cudaSuccess) return bail(e, "memset");
     if ((e = cudaMemset(p->d_out, 0, sizeof(PoolOutput) * d.max_episodes)) != cudaSuccess) return bail(e, "memset");
     // one link table for all episodes, keyed by slot * 2^22 + cell
@@ -446,7 +475,9 @@ ffs_status ffs_pool_create(const ffs_pool_desc *desc, ffs_pool **out)
     case FFS_STORAGE_F16: p->grid_link = p->sms * pool_link_cells_blocks_per_sm<__half>(); break;
     default: p->grid_link = p->sms * pool_link_cells_blocks_per_sm<__nv_bfloat16>(); break;
     }
-    if ((e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+    for (int b = 0; b < 2; ++b)
+        if ((e = cudaEventCreateWithFlags(&p->done[b], cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+    if ((e = cudaEventCreateWithFlags(&p->act_sent, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
     if ((e = cudaEventCreate(&p->ev0)) != cudaSuccess) return bail(e, "event");
     if ((e = cudaEventCreate(&p->ev1)) != cudaSuccess) return bail(e, "event");
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(e, "create sync");
@@ -461,14 +492,18 @@ ffs_status ffs_pool_destroy(ffs_pool *p)
     for (auto &row : p->graph)
         for (auto &g : row)
             if (g) cudaGraphExecDestroy(g);
-    if (p->done) cudaEventDestroy(p->done);
+    for (int b = 0; b < 2; ++b)
+        if (p->done[b]) cudaEventDestroy(p->done[b]);
+    if (p->act_sent) cudaEventDestroy(p->act_sent);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     cudaFree(p->lt.keys); cudaFree(p->lt.links); cudaFree(p->lt.list); cudaFree(p->lt.count); cudaFree(p->owner);
     cudaFree(p->d_eps); cudaFree(p->d_prm); cudaFree(p->d_act); cudaFree(p->d_out); cudaFree(p->arena_mem);
-    if (p->h_prm) cudaFreeHost(p->h_prm);
+    for (int b = 0; b < 2; ++b)
+        if (p->h_prm[b]) cudaFreeHost(p->h_prm[b]);
     if (p->h_act) cudaFreeHost(p->h_act);
-    if (p->h_out) cudaFreeHost(p->h_out);
+    for (int b = 0; b < 2; ++b)
+        if (p->h_out[b]) cudaFreeHost(p->h_out[b]);
     if (p->own_stream && p->st) cudaStreamDestroy(p->st);
     delete p;
     return FFS_OK;
@@ -603,7 +638,8 @@ ffs_status ffs_pool_admit(ffs_pool *p, const ffs_episode_desc *ep, int *slot_out
     // the admission complete before the caller reuses its arrays anyway
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
         return undo(fail(FFS_ERR_CUDA, std::string("admission: ") + cudaGetErrorString(e)));
-    p->inflight = false;
+    p->inflight[0] = p->inflight[1] = false;
+    p->act_pending = false;
     p->order.push_back(si);
     p->act_dirty = true;
     *slot_out = si;
@@ -653,9 +689,12 @@ ffs_status ffs_pool_tune(ffs_pool *p)
 ffs_status ffs_pool_advance(ffs_pool *p)
 {
     if (!p) return fail(FFS_ERR_INVALID_ARGUMENT, "null pool");
-    ffs_status r = wait_idle(p);
-    if (r != FFS_OK) return r;
     if (p->order.empty()) return FFS_OK;
+    // this step uses pinned buffer nb; wait only for the step that used it
+    // last (two steps back), not for the previous one
+    const int nb = (int)(p->advances & 1);
+    ffs_status r = wait_buffer(p, nb);
+    if (r != FFS_OK) return r;
     const int64_t cells = mix_cells(p);
     if (p->tuned_cells == 0 || cells > 2 * p->tuned_cells || 2 * cells < p->tuned_cells) {
         r = tune(p);
@@ -668,13 +707,16 @@ ffs_status ffs_pool_advance(ffs_pool *p)
     const int S = p->d.substeps;
     for (size_t a = 0; a < p->order.size(); ++a) {
         Slot &s = p->slots[p->order[a]];
-        PoolParams &P = p->h_prm[a];
+        PoolParams &P = p->h_prm[nb][a];
         std::memcpy(P.actions, s.actions, sizeof(P.actions));
         for (int j = 0; j < S; ++j) wave_phase(s.omega_wave, s.t0, s.dt, s.q + j, &P.sb[j], &P.cb[j]);
     }
-    POOL_CK(cudaMemcpyAsync(p->d_prm, p->h_prm, sizeof(PoolParams) * p->order.size(), cudaMemcpyHostToDevice, p->st));
+    POOL_CK(cudaMemcpyAsync(p->d_prm, p->h_prm[nb], sizeof(PoolParams) * p->order.size(), cudaMemcpyHostToDevice,
+                            p->st));
     cudaGraphExec_t &g = p->graph[p->shape][p->parity];
     if (!g) {
+        // first use of this (shape, parity): capture with the stream idle
+        if ((r = wait_idle(p)) != FFS_OK) return r;
         switch (p->d.storage) {
         case FFS_STORAGE_F32: r = capture<float>(p, p->shape, p->parity, &g); break;
         case FFS_STORAGE_F16: r = capture<__half>(p, p->shape, p->parity, &g); break;
@@ -683,9 +725,11 @@ ffs_status ffs_pool_advance(ffs_pool *p)
         if (r != FFS_OK) return r;
     }
     POOL_CK(cudaGraphLaunch(g, p->st));
-    POOL_CK(cudaMemcpyAsync(p->h_out, p->d_out, sizeof(PoolOutput) * p->slots.size(), cudaMemcpyDeviceToHost, p->st));
-    POOL_CK(cudaEventRecord(p->done, p->st));
-    p->inflight = true;
+    POOL_CK(cudaMemcpyAsync(p->h_out[nb], p->d_out, sizeof(PoolOutput) * p->slots.size(), cudaMemcpyDeviceToHost,
+                            p->st));
+    POOL_CK(cudaEventRecord(p->done[nb], p->st));
+    p->inflight[nb] = true;
+    p->last = nb;
     p->parity ^= (S & 1);
     for (int si : p->order) p->slots[si].q += S;
     ++p->advances;
@@ -699,7 +743,7 @@ ffs_status ffs_pool_collect(ffs_pool *p, int slot, ffs_pool_output *out, double 
     ffs_status r = wait_idle(p);
     if (r != FFS_OK) return r;
     static_assert(sizeof(PoolOutput) == sizeof(ffs_pool_output), "output record layout");
-    if (out) std::memcpy(out, p->h_out + slot, sizeof(ffs_pool_output));
+    if (out) std::memcpy(out, p->h_out[p->last] + slot, sizeof(ffs_pool_output));
     if (forces) {
         const Slot &s = p->slots[slot];
         POOL_CK(cudaMemcpyAsync(forces, s.dev.force, sizeof(double) * 2 * s.nv, cudaMemcpyDeviceToHost, p->st));
@@ -716,7 +760,7 @@ ffs_status ffs_pool_collect_many(ffs_pool *p, int n, const int *slots, ffs_pool_
             return fail(FFS_ERR_INVALID_ARGUMENT, "no such episode: slot " + std::to_string(slots[i]));
     ffs_status r = wait_idle(p);
     if (r != FFS_OK) return r;
-    for (int i = 0; i < n; ++i) std::memcpy(out + i, p->h_out + slots[i], sizeof(ffs_pool_output));
+    for (int i = 0; i < n; ++i) std::memcpy(out + i, p->h_out[p->last] + slots[i], sizeof(ffs_pool_output));
     return FFS_OK;
 }
 

@@ -401,6 +401,110 @@ def serve(pool: Pool, specs: list[EpisodeSpec], iterations: int, initial: int, a
     }
 
 
+def serve_pipelined(pools: list, specs: list[EpisodeSpec], iterations: int, initial: int, arrivals_per_iter: float,
+                    seed: int = 0, warmup_iterations: int = 0) -> dict:
+    """serve() with the live episodes split over several pools that step in
+    turn, so that the host's work on one group's outputs (and the next
+    actions, admissions and evictions) overlaps the GPU's control step of
+    the others.  Each pool has its own stream; ffs_pool_advance returns at
+    once, so every group's step is queued while the host serves the next.
+
+    One loop iteration serves one group: collect its last control step,
+    retire finished or diverged episodes, admit queued ones (keeping the
+    groups even), set the next actions and advance.  `arrivals_per_iter` is
+    the arrival rate per control step of the whole set, spread over the
+    groups' iterations.  Latency is measured as in serve(): from action
+    submission to the output being on the host.
+    """
+    G = len(pools)
+    rng = np.random.default_rng(seed)
+    feed = deque(specs)
+    queue: deque = deque()
+    live: list[dict] = [dict() for _ in range(G)]
+    pending = [False] * G
+    for _ in range(min(initial, len(feed))):
+        sp = feed.popleft()
+        queue.append((sp, int(rng.integers(0, max(1, sp.length)))))
+    lat: list[float] = []
+    conc: list[int] = []
+    steps = finished = diverged = refused = 0
+    t_begin = None
+    for it in range(iterations + warmup_iterations):
+        if it == warmup_iterations:
+            t_begin = time.perf_counter()
+            lat.clear()
+            conc.clear()
+            steps = 0
+        g = it % G
+        pool, lv = pools[g], live[g]
+        # outputs of this group's last control step (queued G iterations ago)
+        cont, acts = [], []
+        if pending[g]:
+            slots = list(lv)
+            status = pool.collect_many(slots)["status"]
+            t = time.perf_counter()
+            for slot, stat in zip(slots, status):
+                st = lv[slot]
+                lat.append(t - st.submitted)
+                steps += 1
+                st.done_steps += 1
+                if int(stat) & A.STATUS_NONFINITE:
+                    diverged += 1
+                    pool.evict(slot)
+                    del lv[slot]
+                elif st.done_steps >= st.spec.length:
+                    finished += 1
+                    pool.evict(slot)
+                    del lv[slot]
+                else:
+                    cont.append(slot)
+                    acts.append(st.rng.uniform(-1.0, 1.0, pool.num_actions).astype(np.float32))
+            pending[g] = False
+        for _ in range(int(rng.poisson(arrivals_per_iter / G)) if it else 0):
+            if feed:
+                queue.append((feed.popleft(), 0))
+        # admit while this group holds fewer than its share of live and queued episodes
+        share = -(-(sum(len(x) for x in live) + len(queue)) // G)
+        while queue and len(lv) < share:
+            sp, done = queue[0]
+            slot = pool.admit(sp)
+            if slot is None:
+                refused += 1
+                break
+            queue.popleft()
+            er = np.random.default_rng(sp.seed)
+            cont.append(slot)
+            acts.append(er.uniform(-1.0, 1.0, pool.num_actions).astype(np.float32))
+            lv[slot] = _Live(sp, er, done, 0.0)
+        if not lv:
+            if not feed and not queue and not any(live):
+                break
+            continue
+        conc.append(sum(len(x) for x in live))
+        pool.set_actions(cont, np.stack(acts))
+        now = time.perf_counter()
+        for slot in cont:
+            lv[slot].submitted = now
+        pool.advance()
+        pending[g] = True
+    for g, pool in enumerate(pools):
+        if pending[g]:
+            pool.collect_many(list(live[g]))
+    wall = time.perf_counter() - (t_begin if t_begin is not None else time.perf_counter())
+    for g, pool in enumerate(pools):
+        for slot in list(live[g]):
+            pool.evict(slot)
+    lat_ms = np.array(lat) * 1e3
+    return {
+        "env_steps": steps, "seconds": wall, "env_steps_per_s": steps / wall if wall > 0 else 0.0,
+        "p50_ms": float(np.percentile(lat_ms, 50)) if lat else None,
+        "p99_ms": float(np.percentile(lat_ms, 99)) if lat else None,
+        "concurrency_mean": float(np.mean(conc)) if conc else 0.0,
+        "concurrency_min": int(np.min(conc)) if conc else 0, "concurrency_max": int(np.max(conc)) if conc else 0,
+        "finished": finished, "diverged": diverged, "admission_waits": refused, "groups": G,
+    }
+
+
 def plain_rate(specs: list[EpisodeSpec], control_steps: int, substeps: int = 10, min_seconds: float = 0.0) -> dict:
     """Plain per-episode path over `specs`, one episode at a time: env-steps/s
     and per-step latency percentiles (each control step ends with a host sync).

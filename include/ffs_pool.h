@@ -126,10 +126,15 @@ ffs_status ffs_pool_set_actions(ffs_pool *pool, int n, const int *slots, const f
 
 /* Launches one control step of every admitted episode; returns without
  * waiting.  The first call after the mix changed re-uploads the tile table;
- * the first call (and ffs_pool_tune) builds the CUDA graph. */
+ * the first call (and ffs_pool_tune) builds the CUDA graph.  The pinned
+ * parameter and output buffers are double-buffered, so the call does not
+ * wait for the previous control step: it waits only while the step before
+ * that still holds the buffer it refills.  A caller may therefore enqueue
+ * the next control step before collecting the previous one (with actions
+ * that do not depend on its outputs); collect then returns the newer. */
 ffs_status ffs_pool_advance(ffs_pool *pool);
 
-/* Waits for the last control step and returns the slot's outputs.
+/* Waits for the latest control step and returns the slot's outputs.
  * forces (optional): the slot's per-vertex fluid forces of the last
  * substep, (nv, 2) doubles. */
 ffs_status ffs_pool_collect(ffs_pool *pool, int slot, ffs_pool_output *out, double *forces);
