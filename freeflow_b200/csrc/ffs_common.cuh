@@ -148,6 +148,7 @@ enum StatusBits : uint32_t {
     kStatusLinkOverflow = 1u << 1,  // link hash table full; some links were dropped
     kStatusForceRange = 1u << 2,    // a force contribution exceeded the fixed-point range
     kStatusBadElement = 1u << 3,    // element index out of range in the surface
+    kStatusStageTimeout = 1u << 4,  // a staged plane of moments did not arrive within the wait limit
 };
 
 // A post-collision state the step cannot continue from: density not

@@ -39,6 +39,8 @@
 #include "ffs_dense2d.cuh"
 #include "ffs_dense3d.cuh"
 
+#include <cuda.h> // CUtensorMap and its encoder's types (the encoder is fetched at run time)
+
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -325,15 +327,6 @@ __device__ __forceinline__ void add_basis_scaled(float *R, int cx, int cy, int c
     R[7] = fmaf(64.0f * fx * fy, t, R[7]); R[8] = fmaf(16.0f * fy * fz, t, R[8]); R[9] = fmaf(16.0f * fx * fz, t, R[9]);
 }
 
-// R += s * basis(c) for the velocity (cx, cy, cz)
-__device__ __forceinline__ void add_basis(float *R, int cx, int cy, int cz, float s)
-{
-    R[0] += s;
-    R[1] += cx * s; R[2] += cy * s; R[3] += cz * s;
-    R[4] += cx * cx * s; R[5] += cy * cy * s; R[6] += cz * cz * s;
-    R[7] += cx * cy * s; R[8] += cy * cz * s; R[9] += cx * cz * s;
-}
-
 // Bounce-back corrections that the current plane (buf, plane p) allows:
 //   cell p-1 (Rp, mask wp): remove the pulled c_z = -1 populations of wall
 //                           directions (they came from plane p);
@@ -342,15 +335,6 @@ __device__ __forceinline__ void add_basis(float *R, int cx, int cy, int cz, floa
 //   cell p+1 (Rn, mask wn): remove the pulled c_z = +1 ones.
 // Reference rule: FsiCoupling3D.cu:209-222, f_i(x) = max(0, f_inv(i)^rec(x)).
 // Only the set bits are visited (a wall face sets nine of them).
-__device__ __forceinline__ void add_basis_rt(float *R, int cx, int cy, int cz, float s)
-{
-    const float fx = (float)cx, fy = (float)cy, fz = (float)cz;
-    R[0] += s;
-    R[1] = fmaf(fx, s, R[1]); R[2] = fmaf(fy, s, R[2]); R[3] = fmaf(fz, s, R[3]);
-    R[4] = fmaf(fx * fx, s, R[4]); R[5] = fmaf(fy * fy, s, R[5]); R[6] = fmaf(fz * fz, s, R[6]);
-    R[7] = fmaf(fx * fy, s, R[7]); R[8] = fmaf(fy * fz, s, R[8]); R[9] = fmaf(fx * fz, s, R[9]);
-}
-
 // R'' += basis(c_i) w_i max(0, F_inv(i)(x)) (scaled as above) for every wall
 // direction i in w, with the cell's own unweighted populations read from the
 // current plane.
@@ -390,6 +374,64 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
         }
     }
 }
+
+// ------------------------------------------------ staged moments (variant 3)
+// The moments of each halo plane come into shared memory by one TMA tiled
+// copy (cp.async.bulk.tensor, no multicast) two planes ahead, into one of two
+// stages, each with an mbarrier that the copy's bytes complete.  The box is
+// 4D (x, y, z, moment) over the SoA moment planes: kBX cells wide from
+// x0 - kAlign (a 16-byte boundary, as the tiled copy requires), the 10 rows
+// y0 - 1 .. y0 + 8, one plane, all 10 moments.  Cells outside the grid in x
+// or y arrive as zeros; the halo cells that lie there take the reference's
+// wrapped or clamped source with plain loads instead (halo_index).
+template <typename T> struct Stage {
+    static constexpr int kAlign = 16 / (int)sizeof(T);   // elements per 16 bytes
+    static constexpr int kOff = kAlign - 1;              // box x of halo x 0
+    static constexpr int kBX = kHX + 2 * kAlign - 2;     // 40 (FP32) or 48 (16-bit): covers halo x 0..33
+    static constexpr int kElems = kBX * D3::kHY * 10;
+    static constexpr uint32_t kBytes = (uint32_t)(kElems * sizeof(T));
+    static_assert(kBX * sizeof(T) % 16 == 0, "the box's inner extent must be a multiple of 16 bytes");
+    static_assert(kBytes % 128 == 0, "stages start on 128-byte boundaries");
+    // shared-memory layout after the two population planes
+    static constexpr size_t kBase = (D3::kSmemBytes + 127) / 128 * 128;
+    static constexpr size_t kBars = kBase + 2 * (size_t)kBytes;
+    static constexpr size_t kSmem = kBars + 2 * sizeof(uint64_t);
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// generic-proxy accesses of shared memory before async-proxy (TMA) ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                 ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+                 "r"(smem_u32(bar))
+                 : "memory");
+}
+// polls of a stage's barrier before the kernel gives up on it (status bit
+// kStatusStageTimeout; each poll may itself wait a little in hardware)
+constexpr uint32_t kStageWaitPolls = 1u << 22;
 } // namespace
 
 // MINB = CTAs per SM the register budget is cut for; launch_dense3d times the
@@ -401,10 +443,15 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
 // PAIRED: the paired shared-memory layout with packed c_z = -1 / +1
 // arithmetic (variant 2); otherwise one float plane per population
 // (variants 0 and 1).
-template <typename T, int MINB, bool IDX32, bool PAIRED>
-__global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T> g, int zchunk)
+// STAGE: the halo planes' moments are staged in shared memory by TMA copies
+// through `tmap` (variant 3; IDX32 and PAIRED only); otherwise each thread
+// loads its halo cells' moments one plane ahead into registers.
+template <typename T, int MINB, bool IDX32, bool PAIRED, bool STAGE>
+__global__ void __launch_bounds__(D3::kThreads, MINB)
+    dense3d_kernel(GridArgs<T> g, int zchunk, const __grid_constant__ CUtensorMap tmap)
 {
-    extern __shared__ __align__(16) float smem[];
+    static_assert(!STAGE || (IDX32 && PAIRED), "staging is built for the paired 32-bit-index kernel");
+    extern __shared__ __align__(128) float smem[];
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
     const int zb = blockIdx.z * zchunk;
@@ -461,7 +508,13 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     T mA[10], mB[10];
     uint32_t hA = 0, hB = 0; // node types of the two halo cells (bounce-back cells get zero slots)
     auto load_plane = [&](int z) {
-        if constexpr (IDX32) {
+        if constexpr (STAGE) {
+            // moments arrive by the staged copies; the halo cells' node types
+            // still come one plane ahead
+            const uint32_t zo = (uint32_t)halo_index(z, g.nz, wz) * (uint32_t)nxy;
+            hA = g.flags[zo + off_own] & kTypeMask;
+            if (has_ring) hB = g.flags[zo + off_ring] & kTypeMask;
+        } else if constexpr (IDX32) {
             const uint32_t zo = (uint32_t)halo_index(z, g.nz, wz) * (uint32_t)nxy;
             const uint32_t io = zo + off_own, ir = zo + off_ring;
 #pragma unroll
@@ -517,7 +570,7 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     const float ring_sx = tid < 74 ? 1.0f : -1.0f;                 // columns: c_x of the fed populations
     const int ring_kx = tid < 74 ? 2 : 0;                          // their kx = c_x + 1
     const int ring_kxo = ring_kx * kHalo;                          // and its plane offset
-    auto recon_ring = [&](float *buf, bool zero) {
+    auto recon_ring = [&](float *buf, const T *raw, bool zero) {
         const int c = c_ring;
         if (zero) {
             if constexpr (PAIRED) {
@@ -528,21 +581,21 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
                     else if (ring_kind == 1) store_pair(buf, k * kHalo + c, z2, 0.0f);
                     else store_pair(buf, (ring_kx + 3 * k) * kHalo + c, z2, 0.0f);
                 }
-                return;
+            } else {
+#pragma unroll
+                for (int kz = 0; kz < 3; ++kz)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        if (ring_kind == 0) buf[set_of(k, 2, kz) * kHalo + c] = 0.0f;
+                        else if (ring_kind == 1) buf[set_of(k, 0, kz) * kHalo + c] = 0.0f;
+                        else buf[set_of(0, k, kz) * kHalo + ring_kxo + c] = 0.0f;
+                    }
             }
-#pragma unroll
-            for (int kz = 0; kz < 3; ++kz)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if (ring_kind == 0) buf[set_of(k, 2, kz) * kHalo + c] = 0.0f;
-                    else if (ring_kind == 1) buf[set_of(k, 0, kz) * kHalo + c] = 0.0f;
-                    else buf[set_of(0, k, kz) * kHalo + ring_kxo + c] = 0.0f;
-                }
             return;
         }
         float m[10];
 #pragma unroll
-        for (int k = 0; k < 10; ++k) m[k] = from_storage<3, T>(k, mB[k]);
+        for (int k = 0; k < 10; ++k) m[k] = from_storage<3, T>(k, raw[k]);
         decode_moments<3, T>(m, g.codec);
         Coef3V<float> cf;
         cf.make(m);
@@ -561,10 +614,62 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
     };
     // plane p's halo cells; bounce-back cells get zero slots unless they lie
     // beyond a high face
+    // Staging (STAGE): stage s of plane q is (q - zb + 1) & 1, its use
+    // count (q - zb + 1) >> 1 the barrier phase to wait for.
+    using SG = Stage<T>;
+    T *stage_mem = reinterpret_cast<T *>(reinterpret_cast<char *>(smem) + SG::kBase);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(smem) + SG::kBars);
+    bool stage_ok = true;
+    // halo cells outside the grid in x or y come by plain loads
+    auto outside_xy = [&](int c) {
+        const int hx = x0 + c % kHX - 1, hy = y0 + c / kHX - 1;
+        return hx < 0 || hx >= g.nx || hy < 0 || hy >= g.ny;
+    };
+    const bool own_direct = outside_xy(c_own), ring_direct = outside_xy(c_ring);
+    auto issue_plane = [&](int q) { // thread 0 only
+        const int sidx = (q - zb + 1) & 1;
+        mbar_expect_tx(&bars[sidx], SG::kBytes);
+        tma_load_4d(stage_mem + (size_t)sidx * SG::kElems, &tmap, &bars[sidx], x0 - SG::kAlign, y0 - 1,
+                    halo_index(q, g.nz, wz), 0);
+    };
+    auto fetch = [&](int q, int c, bool direct, uint32_t off, T (&raw)[10]) {
+        if (direct) {
+            const uint32_t io = (uint32_t)halo_index(q, g.nz, wz) * (uint32_t)nxy + off;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) raw[k] = g.src[io + (uint32_t)k * g.ncell];
+        } else {
+            const T *st = stage_mem + (size_t)((q - zb + 1) & 1) * SG::kElems;
+            const int e = (c / kHX) * SG::kBX + c % kHX + SG::kOff;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) raw[k] = st[k * (D3::kHY * SG::kBX) + e];
+        }
+    };
     auto recon_plane = [&](float *buf, int p) {
         const bool zhi = !wz && p >= g.nz;
-        recon_cell(buf, mA, is_bounce_back<3>(hA) && !(own_hi || zhi), c_own);
-        if (has_ring) recon_ring(buf, is_bounce_back<3>(hB) && !(ring_hi || zhi));
+        if constexpr (STAGE) {
+            const int sidx = (p - zb + 1) & 1;
+            const uint32_t parity = (uint32_t)((p - zb + 1) >> 1) & 1u;
+            if (stage_ok) {
+                uint32_t polls = 0;
+                while (!mbar_try_wait(&bars[sidx], parity)) {
+                    if (++polls >= kStageWaitPolls) {
+                        atomicOr(g.status, kStatusStageTimeout);
+                        stage_ok = false;
+                        break;
+                    }
+                }
+            }
+            T raw[10];
+            fetch(p, c_own, own_direct, off_own, raw);
+            recon_cell(buf, raw, is_bounce_back<3>(hA) && !(own_hi || zhi), c_own);
+            if (has_ring) {
+                fetch(p, c_ring, ring_direct, off_ring, raw);
+                recon_ring(buf, raw, is_bounce_back<3>(hB) && !(ring_hi || zhi));
+            }
+        } else {
+            recon_cell(buf, mA, is_bounce_back<3>(hA) && !(own_hi || zhi), c_own);
+            if (has_ring) recon_ring(buf, mB, is_bounce_back<3>(hB) && !(ring_hi || zhi));
+        }
     };
     auto flag_at = [&](int z) -> uint32_t {
         return (inside && z >= zb && z < ze) ? (uint32_t)g.flags[cell_at(z)] : 0u;
@@ -592,6 +697,13 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         const bool upd_n = is_updated(fn & kTypeMask) && !(fn & kBitLink);
         const uint32_t wn = (upd_n && (fn & (kBitNearWall | kBitOutletSrc))) ? g.wallmask[cell_at(p + 1)] : 0u;
         __syncthreads();
+        if constexpr (STAGE) {
+            // every thread has read plane p's stage: refill it with plane p + 2
+            if (tid == 0 && stage_ok && p + 2 <= ze) {
+                fence_proxy_async();
+                issue_plane(p + 2);
+            }
+        }
         if (inside) {
             constexpr uint32_t kWall = wall_bits_mask<3>();
             // the cell at z = p - 1 is complete: collide, store, feed outlets
@@ -656,6 +768,18 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         wp = wc; wc = wn;
     };
 
+    if constexpr (STAGE) {
+        if (tid == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            mbar_init_fence();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            issue_plane(zb - 1);
+            issue_plane(zb);
+        }
+    }
     load_plane(zb - 1);
     int p = zb - 1;
     for (; p + 1 <= ze; p += 2) {
@@ -663,6 +787,18 @@ __global__ void __launch_bounds__(D3::kThreads, MINB) dense3d_kernel(GridArgs<T>
         plane(p + 1, Y, X); // completes Y (z = p);   Y := z = p+2
     }
     if (p <= ze) plane(p, X, Y);
+    if constexpr (STAGE) {
+        // after a wait gave up, wait (bounded) for the copies still in flight
+        // into this CTA's shared memory before it exits
+        if (!stage_ok && tid == 0) {
+            for (int q = max(zb - 1, ze - 1); q <= ze; ++q) {
+                const int sidx = (q - zb + 1) & 1;
+                const uint32_t parity = (uint32_t)((q - zb + 1) >> 1) & 1u;
+                for (uint32_t polls = 0; polls < kStageWaitPolls && !mbar_try_wait(&bars[sidx], parity); ++polls) {
+                }
+            }
+        }
+    }
 }
 
 // CTAs of `kernel` resident on the current device at once (SMs x occupancy),
@@ -713,19 +849,60 @@ static int choose_zchunks(int tiles, int nz, int slots)
     return best;
 }
 
-template <typename T, int MINB, bool IDX32, bool PAIRED> struct Dense3dLaunchAs {
-    static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
+// cuTensorMapEncodeTiled, fetched from the driver once (the library links
+// only the runtime).  Null when the driver does not offer it.
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled tensor_map_encoder()
+{
+    static const EncodeTiled fn = []() -> EncodeTiled {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &ptr, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<EncodeTiled>(ptr);
+    }();
+    return fn;
+}
+
+// The staged copies' tensor map over the source moments: 4D (x, y, z,
+// moment), box (kBX, 10, 1, 10), zeros outside the grid.  False when the
+// grid cannot be staged: a row of moments must be a multiple of 16 bytes
+// (nx a multiple of 4 in FP32, of 8 in 16-bit storage), indices must fit in
+// 32 bits, or the encoder refuses the shape.
+template <typename T> static bool stage_map(const GridArgs<T> &g, CUtensorMap &map)
+{
+    if (((size_t)g.nx * sizeof(T)) % 16 != 0 || reinterpret_cast<uintptr_t>(g.src) % 16 != 0) return false;
+    if (10ull * g.ncell > 0xFFFFFFFFull) return false;
+    const EncodeTiled enc = tensor_map_encoder();
+    if (!enc) return false;
+    const size_t es = sizeof(T);
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, 10};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.nx * es, (cuuint64_t)g.nx * g.ny * es, (cuuint64_t)g.ncell * es};
+    const cuuint32_t box[4] = {(cuuint32_t)Stage<T>::kBX, (cuuint32_t)D3::kHY, 1, 10};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    const CUtensorMapDataType dt = es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    return enc(&map, dt, 4, const_cast<T *>(g.src), dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, int MINB, bool IDX32, bool PAIRED, bool STAGE> struct Dense3dLaunchAs {
+    static cudaError_t run(const GridArgs<T> &g, cudaStream_t s, const CUtensorMap &map)
     {
         int slots = 0;
-        constexpr size_t smem = D3::kSmemBytes;
-        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_kernel<T, MINB, IDX32, PAIRED>),
+        constexpr size_t smem = STAGE ? Stage<T>::kSmem : D3::kSmemBytes;
+        cudaError_t e = resident_slots(reinterpret_cast<const void *>(dense3d_kernel<T, MINB, IDX32, PAIRED, STAGE>),
                                        D3::kThreads, smem, slots);
         if (e != cudaSuccess) return e;
         int tx = (g.nx + kTX - 1) / kTX, ty = (g.ny + kTY - 1) / kTY;
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
         dim3 grid(tx, ty, (g.nz + zchunk - 1) / zchunk);
-        dense3d_kernel<T, MINB, IDX32, PAIRED><<<grid, D3::kThreads, smem, s>>>(g, zchunk);
+        dense3d_kernel<T, MINB, IDX32, PAIRED, STAGE><<<grid, D3::kThreads, smem, s>>>(g, zchunk, map);
         return cudaGetLastError();
     }
 };
@@ -735,15 +912,31 @@ template <typename T, int MINB, bool IDX32, bool PAIRED> struct Dense3dLaunchAs 
 template <typename T, int MINB, bool PAIRED> struct Dense3dLaunch {
     static cudaError_t run(const GridArgs<T> &g, cudaStream_t s)
     {
+        const CUtensorMap none{};
         const char *force64 = std::getenv("FFS_DENSE3D_INDEX64");
         if (10ull * g.ncell <= 0xFFFFFFFFull && !(force64 && force64[0] == '1'))
-            return Dense3dLaunchAs<T, MINB, true, PAIRED>::run(g, s);
-        return Dense3dLaunchAs<T, MINB, false, PAIRED>::run(g, s);
+            return Dense3dLaunchAs<T, MINB, true, PAIRED, false>::run(g, s, none);
+        return Dense3dLaunchAs<T, MINB, false, PAIRED, false>::run(g, s, none);
     }
 };
 
+// Variant 3: staged moments; grids that cannot be staged run variant 2.
+template <typename T> static cudaError_t launch_staged(const GridArgs<T> &g, cudaStream_t s)
+{
+    CUtensorMap map;
+    if (!stage_map(g, map)) return Dense3dLaunch<T, 2, true>::run(g, s);
+    return Dense3dLaunchAs<T, 2, true, true, true>::run(g, s, map);
+}
 
-template <typename T> bool dense3d_has_variant(int v) { return v >= 0 && v < kDense3dVariants; }
+
+template <typename T> bool dense3d_has_variant(int v, const GridArgs<T> &g)
+{
+    if (v == 3) {
+        CUtensorMap map;
+        return stage_map(g, map);
+    }
+    return v >= 0 && v < kDense3dVariants;
+}
 
 template <typename T>
 cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
@@ -751,6 +944,7 @@ cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
     switch (variant) {
     case 1: return Dense3dLaunch<T, 3, false>::run(g, s);
     case 2: return Dense3dLaunch<T, 2, true>::run(g, s);
+    case 3: return launch_staged<T>(g, s);
     default: return Dense3dLaunch<T, 2, false>::run(g, s);
     }
 }
@@ -763,7 +957,7 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     // FFS_DENSE3D_VARIANT pins the variant (tests run every variant this way)
     if (const char *pin = std::getenv("FFS_DENSE3D_VARIANT")) {
         const int v = std::atoi(pin);
-        if (dense3d_has_variant<T>(v)) return v;
+        if (dense3d_has_variant<T>(v, g)) return v;
     }
     cudaEvent_t a, b;
     cudaEventCreate(&a);
@@ -773,7 +967,7 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     // the scalar layout for two and three CTAs per SM and the paired layout,
     // which all round identically
     for (int v = 0; v < kDense3dVariants; ++v) {
-        if (!dense3d_has_variant<T>(v)) continue;
+        if (!dense3d_has_variant<T>(v, g)) continue;
         if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue; // warm-up
         cudaEventRecord(a, s);
         for (int r = 0; r < 3; ++r) launch_dense3d<T>(g, s, v);

@@ -233,7 +233,9 @@ ffs_status ffs_lbm_fill_solid(ffs_lbm *grid, const ffs_surface *surface, void *s
 /* Reads (and optionally clears) the device status word; synchronises
  * `stream`.  Bits: 1 a fluid update produced a non-positive or non-finite
  * density or a non-finite velocity, 2 link table overflow, 4 force out of
- * fixed-point range, 8 element index out of range. */
+ * fixed-point range, 8 element index out of range, 16 a staged plane of
+ * moments did not reach shared memory within the dense pass's wait limit
+ * (the step's results are invalid; not expected to happen). */
 ffs_status ffs_lbm_get_status(ffs_lbm *grid, uint32_t *status, int clear, void *stream);
 
 /* Grid facts: cell count, moments per cell, directions, omega, Cf. */

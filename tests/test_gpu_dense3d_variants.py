@@ -3,7 +3,9 @@ per grid by speed, so each must pass the parity cases on its own).
 
 Variants: 0 and 1 are the single-plane z-march built for two and three CTAs
 per SM; 2 is the two-CTA march with the paired shared-memory layout and
-packed c_z = -1 / +1 arithmetic.
+packed c_z = -1 / +1 arithmetic; 3 is variant 2 with each halo plane's
+moments staged in shared memory by TMA copies (32-bit indices only; grids
+whose rows are not a multiple of 16 bytes run variant 2).
 Tolerances are those of test_gpu_parity.py: 2e-6 against the ref32 oracle,
 4e-6 next to walls (bounce-back added as a correction), 5e-6 against FP64.
 """
@@ -19,7 +21,7 @@ pytestmark = pytest.mark.gpu
 # (variant, index width): the single-plane variants run with 32-bit indices on
 # grids of up to 429 M cells and 64-bit ones beyond; FFS_DENSE3D_INDEX64 forces
 # the 64-bit path here
-VARIANTS = [(0, 32), (1, 32), (2, 32), (0, 64), (1, 64), (2, 64)]
+VARIANTS = [(0, 32), (1, 32), (2, 32), (3, 32), (0, 64), (1, 64), (2, 64)]
 
 
 @pytest.fixture(params=VARIANTS, ids=lambda v: f"v{v[0]}-i{v[1]}")
@@ -115,7 +117,7 @@ def test_tuned_variants_round_identically(cuda, monkeypatch, storage):
 
     wl = W.swimmer_3d(nx=64, ny=32, nz=32, body_frac=0.4, nlat=16, nlon=24, seed=4)
     out = []
-    for v in ("0", "1", "2"):
+    for v in ("0", "1", "2", "3"):
         monkeypatch.setenv("FFS_DENSE3D_VARIANT", v)
         g, s = make_gpu(wl, storage)
         for k in range(6):
