@@ -174,11 +174,15 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
     static_assert(Q <= G, "one lane per direction");
     const int lane = threadIdx.x & (G - 1);
     const unsigned full = 0xffffffffu;
-    const long long nxy = (long long)g.nx * g.ny;
+    // cell indices are 32-bit (the link table keys them so), and so is every
+    // index formed from them here
+    const uint32_t nx = (uint32_t)g.nx, nxy = nx * (uint32_t)g.ny;
     const bool wx = g.periodic & 1, wy = g.periodic & 2, wz = g.periodic & 4;
-    const int x = (int)(cell % g.nx);
-    const int y = (int)((cell / g.nx) % g.ny);
-    const int z = (int)(cell / nxy);
+    const uint32_t row = cell / nx;
+    const int x = (int)(cell - row * nx);
+    const uint32_t z32 = row / (uint32_t)g.ny;
+    const int y = (int)(row - z32 * (uint32_t)g.ny);
+    const int z = (int)z32;
     const uint8_t f8 = g.flags[cell];
     const bool upd = valid && is_updated(f8 & kTypeMask);
     float mc[NM];
@@ -197,8 +201,9 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
             dir_vec<DIM>(i, cx, cy, cz);
             const int x1 = x - cx, y1 = y - cy, z1 = z - cz;
             const bool notCross = x1 >= 0 && x1 < g.nx && y1 >= 0 && y1 < g.ny && z1 >= 0 && z1 < g.nz;
-            const int ax = (x1 + g.nx) % g.nx, ay = (y1 + g.ny) % g.ny, az = (z1 + g.nz) % g.nz;
-            const uint32_t ib = (uint32_t)((long long)az * nxy + (long long)ay * g.nx + ax);
+            // the wrapped neighbour (x1, y1, z1 are within one cell of the grid)
+            auto wrap1 = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
+            const uint32_t ib = (uint32_t)wrap1(z1, g.nz) * nxy + (uint32_t)wrap1(y1, g.ny) * nx + (uint32_t)wrap1(x1, g.nx);
             bool done = false;
             // a wall neighbour: bounce-back, no link (with wall_stream in 2D, the
             // reference's 2D kernel: the ordinary pull, no link either)
@@ -270,7 +275,7 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
             if (!done) {
                 // ordinary pull from the upstream halo cell (halo_index)
                 const int sx = halo_index(x1, g.nx, wx), sy = halo_index(y1, g.ny, wy), sz = halo_index(z1, g.nz, wz);
-                const uint32_t sidx = (uint32_t)((long long)sz * nxy + (long long)sy * g.nx + sx);
+                const uint32_t sidx = (uint32_t)sz * nxy + (uint32_t)sy * nx + (uint32_t)sx;
                 float mn[NM];
                 load_moments<DIM, T>(mn, g.src, g.ncell, sidx, g.codec);
                 Coef<DIM> nc;
