@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(TX * TY) pool_dense_kernel(const PoolEpisode *
 // code as the tile kernel, so both give the same bits.  Episodes hold fewer
 // than 2^22 cells, so every moment index fits in 32 bits.
 template <typename T, int TX, int CH, int DEPTH>
-__global__ void __launch_bounds__(TX) pool_strip_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
+__global__ void __launch_bounds__(TX, 1024 / TX) pool_strip_kernel(const PoolEpisode *eps, const PoolActive *act, int parity)
 {
     using L = Lattice<2>;
     constexpr int kOut = TX - 2;              // columns a strip updates
