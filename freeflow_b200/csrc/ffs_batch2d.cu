@@ -93,11 +93,15 @@ __global__ void pool_kinematics_kernel(const PoolEpisode *eps, const PoolParams 
 
 // ---------------------------------------------------------------- detect
 // One warp per element of any episode (the single-grid body,
-// detect_element2_warp); the warp finds the element's episode once.
+// detect_element2_warp); the warp finds the element's episode once.  (Giving
+// each warp a contiguous run of elements, so that the episode search runs
+// once per run, measured no faster: the time goes to the link insertions'
+// dependent atomics, not to the search.)
 template <typename T>
 __global__ void __launch_bounds__(256) pool_detect_kernel(const PoolEpisode *eps, const PoolActive *act, LinkTable lt,
                                                           uint32_t *owner, int parity)
 {
+    __shared__ uint32_t queue[8][64]; // per warp: (cell, direction) pairs for the exact test
     const int n = (int)act->n;
     if (n == 0) return;
     const uint32_t total = act->elem_prefix[n];
@@ -110,7 +114,7 @@ __global__ void __launch_bounds__(256) pool_detect_kernel(const PoolEpisode *eps
         const SurfaceArgs sa = episode_surface(e);
         const StepScalars sc{e.cl, e.ct, e.cf};
         detect_element2_warp<T>(g, reinterpret_cast<uint32_t *>(e.flags), lt, sa, sc,
-                                (long long)(ge - act->elem_prefix[a]), e.cell_base, owner, s);
+                                (long long)(ge - act->elem_prefix[a]), queue[threadIdx.x >> 5], e.cell_base, owner, s);
     }
 }
 

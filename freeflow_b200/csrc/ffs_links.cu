@@ -152,9 +152,10 @@ template <typename T>
 __global__ void __launch_bounds__(256) detect_links2_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt,
                                                             SurfaceArgs s, StepScalars sc)
 {
+    __shared__ uint32_t queue[8][64]; // per warp: (cell, direction) pairs for the exact test
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < s.ne; e += nwarps)
-        detect_element2_warp<T>(g, flag_words, lt, s, sc, e);
+        detect_element2_warp<T>(g, flag_words, lt, s, sc, e, queue[threadIdx.x >> 5]);
 }
 
 // -------------------------------------------------------------- link cells

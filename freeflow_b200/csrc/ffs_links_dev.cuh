@@ -63,14 +63,26 @@ __device__ __forceinline__ void insert_link(const LinkTable &lt, uint32_t *flag_
 // numbered cell * 8 + (l - 1) with cells in row-major order; 32 items are four
 // cells, so a lane keeps one direction and steps its cell by four, carrying
 // the cell's coordinates forward instead of dividing them out.
+//
+// Most pairs cannot cross: a hit needs the element's line to separate the
+// link's two end points (line_intersect's t1 = s2 / (s2 - s1) in (0, 1), with
+// s1, s2 their signed distances).  A cheap prefilter drops a pair only when
+// both end points lie on the same side by more than a hundredth of a cell
+// (times the element's length); then t1 is at least about 7e-3 outside
+// (0, 1), far beyond the exact test's rounding, so the link set is the
+// exact test's.  The surviving pairs are queued in `wq` (64 entries of this
+// warp's shared memory) and the exact, explicitly rounded test runs on 32 of
+// them at a time, so that its lanes are not idle.  Boxes wider or taller than
+// 16,383 cells skip the queue (the packed item holds 14-bit coordinates).
 template <typename T>
 __device__ __forceinline__ void detect_element2_warp(const GridArgs<T> &g, uint32_t *flag_words, const LinkTable &lt,
                                                      const SurfaceArgs &s, const StepScalars &sc, long long e,
-                                                     uint32_t key_base = 0, uint32_t *owner = nullptr,
+                                                     uint32_t *wq, uint32_t key_base = 0, uint32_t *owner = nullptr,
                                                      uint32_t owner_id = 0)
 {
     constexpr int Q = 9;
     const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
     const uint32_t va = s.E[2 * e], vb = s.E[2 * e + 1];
     if (va >= (uint32_t)s.nv || vb >= (uint32_t)s.nv) {
         if (lane == 0) atomicOr(g.status, kStatusBadElement);
@@ -98,22 +110,69 @@ __device__ __forceinline__ void detect_element2_warp(const GridArgs<T> &g, uint3
     const int l = (lane & 7) + 1;
     int cx, cy, cz;
     dir_vec<2>(l, cx, cy, cz);
+    // the exact test of cell (i, j), direction ll, and the insertion on a hit
+    auto exact = [&](int i, int j, int ll) {
+        int dx, dy, dz;
+        dir_vec<2>(ll, dx, dy, dz);
+        const geom::Hit h = geom::isect2(s.V, va, vb, geom::mul((float)i, cl), geom::mul((float)j, cl),
+                                         geom::mul(geom::sub((float)i, (float)dx), cl),
+                                         geom::mul(geom::sub((float)j, (float)dy), cl));
+        if (!h.hit) return;
+        const uint32_t cell = (uint32_t)((long long)j * g.nx + i);
+        insert_link<Q>(lt, flag_words, cell, ll, geom::link_key(h.depth, (uint32_t)e), g.status, key_base, owner,
+                       owner_id);
+    };
     int ci = lane >> 3, cj = 0;
     while (ci >= ext0) { ci -= ext0; ++cj; }
-    for (long long it = lane; it < items; it += 32) {
-        if (it != lane) {
+    if (ext0 > 16383 || ext1 > 16383) {
+        for (long long it = lane; it < items; it += 32) {
+            if (it != lane) {
+                ci += 4;
+                while (ci >= ext0) { ci -= ext0; ++cj; }
+            }
+            exact(lo0 + ci, lo1 + cj, l);
+        }
+        return;
+    }
+    // the element's line: normal (y3 - y4, x4 - x3) through vertex 4; the
+    // prefilter's own rounding is far below its margin
+    const float x3 = s.V[2 * (size_t)va], y3 = s.V[2 * (size_t)va + 1];
+    const float x4 = s.V[2 * (size_t)vb], y4 = s.V[2 * (size_t)vb + 1];
+    const float en0 = y3 - y4, en1 = x4 - x3;
+    const float margin = 1e-2f * cl * sqrtf(en0 * en0 + en1 * en1);
+    const float dstep = cl * (en0 * (float)cx + en1 * (float)cy); // s1 - s2 of this lane's direction
+    const unsigned below = (1u << lane) - 1u;
+    int qn = 0;
+    for (long long base = 0; base < items; base += 32) {
+        if (base != 0) {
             ci += 4;
             while (ci >= ext0) { ci -= ext0; ++cj; }
         }
-        const int i = lo0 + ci, j = lo1 + cj;
-        const geom::Hit h = geom::isect2(s.V, va, vb, geom::mul((float)i, cl), geom::mul((float)j, cl),
-                                         geom::mul(geom::sub((float)i, (float)cx), cl),
-                                         geom::mul(geom::sub((float)j, (float)cy), cl));
-        if (!h.hit) continue;
-        const uint32_t cell = (uint32_t)((long long)j * g.nx + i);
-        insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status, key_base, owner,
-                       owner_id);
+        bool cand = false;
+        if (base + lane < items) {
+            const float s1 = en0 * ((float)(lo0 + ci) * cl - x4) + en1 * ((float)(lo1 + cj) * cl - y4);
+            const float s2 = s1 - dstep;
+            cand = !(fabsf(s1) > margin && fabsf(s2) > margin && ((s1 > 0.0f) == (s2 > 0.0f)));
+        }
+        const unsigned m = __ballot_sync(full, cand);
+        if (cand) wq[qn + __popc(m & below)] = ((uint32_t)cj << 17) | ((uint32_t)ci << 3) | (uint32_t)(l - 1);
+        qn += __popc(m);
+        if (qn >= 32) {
+            __syncwarp();
+            const uint32_t code = wq[lane];
+            __syncwarp();
+            if (lane < qn - 32) wq[lane] = wq[32 + lane];
+            __syncwarp();
+            qn -= 32;
+            exact(lo0 + (int)((code >> 3) & 0x3fffu), lo1 + (int)(code >> 17), (int)(code & 7u) + 1);
+        }
     }
+    __syncwarp();
+    if (lane < qn) {
+        const uint32_t code = wq[lane];
+        exact(lo0 + (int)((code >> 3) & 0x3fffu), lo1 + (int)(code >> 17), (int)(code & 7u) + 1);
+    }
+    __syncwarp();
 }
 
 // Per-vertex force shares of the links of one cell.  Lanes whose links hit
