@@ -61,6 +61,9 @@ template <auto KERNEL> static int resident_grid(int threads)
 // triangle by more than 1% in barycentric terms.  Every remaining pair gets
 // the exact, explicitly rounded test, so the link set does not depend on
 // this enumeration (the table keeps the minimum key per cell and direction).
+// Only a few lanes of a cell pass the prefilter, so the surviving pairs are
+// queued in shared memory (64 entries per warp) and the exact test runs on 32
+// of them at a time; boxes larger than 1024 x 1024 x 128 cells skip the queue.
 template <typename T>
 __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint32_t *flag_words, LinkTable lt,
                                                             SurfaceArgs s, StepScalars sc)
@@ -75,6 +78,9 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
     int cx, cy, cz;
     dir_vec<3>(l, cx, cy, cz);
     const float ccx = (float)cx * cl, ccy = (float)cy * cl, ccz = (float)cz * cl;
+    __shared__ uint32_t queue[8][64]; // per warp: (cell, direction) pairs for the exact test
+    uint32_t *wq = queue[threadIdx.x >> 5];
+    const unsigned full = 0xffffffffu, below = (1u << lane) - 1u;
     for (long long e = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < s.ne; e += nwarps) {
         const uint32_t ia = s.E[3 * e], ib = s.E[3 * e + 1], ic = s.E[3 * e + 2];
         if (ia >= (uint32_t)s.nv || ib >= (uint32_t)s.nv || ic >= (uint32_t)s.nv) {
@@ -107,6 +113,31 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
         const bool reach = fa > margin;              // else: the link runs (nearly) parallel to the plane
         const float sg = a > 0.0f ? 1.0f : -1.0f;
         const float inv_a = reach ? __fdividef(1.0f, a) : 0.0f;
+        // the exact test of cell (i, j, k3), direction ll, and the insertion on a hit
+        auto exact = [&](int i, int j, int k3, int ll) {
+            int dx, dy, dz;
+            dir_vec<3>(ll, dx, dy, dz);
+            float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
+            float p2[3] = {geom::mul(geom::sub((float)i, (float)dx), cl), geom::mul(geom::sub((float)j, (float)dy), cl),
+                           geom::mul(geom::sub((float)k3, (float)dz), cl)};
+            const geom::Hit h = geom::isect3_pre(tr, p1, p2);
+            if (!h.hit) return;
+            const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
+            insert_link<Q>(lt, flag_words, cell, ll, geom::link_key(h.depth, (uint32_t)e), g.status);
+        };
+        const bool queued = hi[0] - lo[0] < 1024 && hi[1] - lo[1] < 1024 && hi[2] - lo[2] < 128;
+        int qn = 0;
+        auto drain = [&](int upto) { // run the exact test on the first `upto` queued pairs
+            __syncwarp();
+            const uint32_t code = wq[lane];
+            __syncwarp();
+            if (lane < qn - upto) wq[lane] = wq[upto + lane];
+            __syncwarp();
+            if (lane < upto)
+                exact(lo[0] + (int)(code & 1023u), lo[1] + (int)((code >> 10) & 1023u), lo[2] + (int)((code >> 20) & 127u),
+                      (int)(code >> 27) + 1);
+            qn -= upto;
+        };
         for (int k3 = lo[2]; k3 <= hi[2]; ++k3) {
             const float pz = (float)k3 * cl - tr.v0[2];
             for (int j = lo[1]; j <= hi[1]; ++j) {
@@ -132,18 +163,22 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
                     } else {
                         cand = !(fabsf(s1) > 2.0f * margin);
                     }
-                    if (!(act && cand)) continue;
-                    float p1[3] = {geom::mul((float)i, cl), geom::mul((float)j, cl), geom::mul((float)k3, cl)};
-                    float p2[3] = {geom::mul(geom::sub((float)i, (float)cx), cl),
-                                   geom::mul(geom::sub((float)j, (float)cy), cl),
-                                   geom::mul(geom::sub((float)k3, (float)cz), cl)};
-                    const geom::Hit h = geom::isect3_pre(tr, p1, p2);
-                    if (!h.hit) continue;
-                    const uint32_t cell = (uint32_t)(((long long)k3 * g.ny + j) * g.nx + i);
-                    insert_link<Q>(lt, flag_words, cell, l, geom::link_key(h.depth, (uint32_t)e), g.status);
+                    cand = act && cand;
+                    if (!queued) {
+                        if (cand) exact(i, j, k3, l);
+                        continue;
+                    }
+                    const unsigned m = __ballot_sync(full, cand);
+                    if (cand)
+                        wq[qn + __popc(m & below)] = (uint32_t)(i - lo[0]) | ((uint32_t)(j - lo[1]) << 10) |
+                                                     ((uint32_t)(k3 - lo[2]) << 20) | ((uint32_t)(l - 1) << 27);
+                    qn += __popc(m);
+                    if (qn >= 32) drain(32);
                 }
             }
         }
+        if (queued && qn > 0) drain(qn);
+        __syncwarp();
     }
 }
 
