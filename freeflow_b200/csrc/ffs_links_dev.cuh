@@ -175,39 +175,37 @@ __device__ __forceinline__ void detect_element2_warp(const GridArgs<T> &g, uint3
     __syncwarp();
 }
 
-// Per-vertex force shares of the links of one cell.  Lanes whose links hit
-// the same element (found with __match_any_sync) are summed with the warp's
-// integer reduction unit (__reduce_add_sync), one value per (vertex slot,
-// component), in 2^-24 fixed point; the group leader then adds each sum, in
-// 2^-32 fixed point, to the vertex accumulator with one 64-bit integer
-// atomic.  Integer sums are associative, so the per-vertex result does not
-// depend on warp, lane or launch order.  A share beyond +-127 lattice units
-// (outside the 2^-24 range of 27 summed int32 shares) is clamped and flagged.
-// Lanes are grouped by (lane group, element): the groups of one warp may
-// update cells of different grids, whose element numbers name different
-// elements and whose accumulators differ.
+// Per-vertex force shares of the links of one cell, added to the vertex
+// accumulators in 2^-32 fixed point with 64-bit integer atomics, one per
+// (link, vertex slot, component).  Integer sums are associative, so the
+// per-vertex result does not depend on warp, lane or launch order.  Each
+// share is first rounded to 2^-24 (as an int32) and then scaled by 2^8,
+// which is exactly what summing the int32 shares of a cell's links to one
+// element and scaling the sum would give; a share beyond +-127 lattice units
+// is clamped and flagged.  (An earlier form summed the links of one element
+// within the warp first, with __match_any_sync and __reduce_add_sync over
+// partial masks; the compiler loops such collectives per group, which cost
+// about 120 instructions per cell, more than the atomics they saved.)
 template <int DIM>
 __device__ __forceinline__ void add_forces_warp(long long *acc, bool active, uint32_t elem, const uint32_t *vert,
                                                 const float (*share)[3], uint32_t *status, uint32_t group = 0)
 {
-    const unsigned full = 0xffffffffu;
-    const unsigned peers = __match_any_sync(full, active ? ((unsigned long long)group << 32) | elem : ~0ull);
-    const int lane = threadIdx.x & 31;
-    const bool leader = active && lane == __ffs(peers) - 1;
+    (void)elem;
+    (void)group;
+    if (!active) return;
 #pragma unroll
     for (int j = 0; j < DIM; ++j)
 #pragma unroll
         for (int k = 0; k < DIM; ++k) {
-            float v = active ? share[j][k] : 0.0f;
+            float v = share[j][k];
             if (!(fabsf(v) < 127.0f)) {
-                if (active) atomicOr(status, kStatusForceRange);
+                atomicOr(status, kStatusForceRange);
                 v = isfinite(v) ? copysignf(127.0f, v) : 0.0f;
             }
             const int q = __float2int_rn(v * 16777216.0f); // 2^24
-            const int sum = (int)__reduce_add_sync(peers, (unsigned)q);
-            if (leader && sum != 0)
+            if (q != 0)
                 atomicAdd(reinterpret_cast<unsigned long long *>(acc + (size_t)vert[j] * DIM + k),
-                          (unsigned long long)((long long)sum * 256)); // 2^24 -> 2^32
+                          (unsigned long long)((long long)q * 256)); // 2^24 -> 2^32
         }
 }
 
