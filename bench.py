@@ -742,11 +742,17 @@ def run_ours(args):
                "copies": "serial: each step's uploads, step and read-back in order on one stream"}
         if not small:
             ems_p = R.max_over_ranks(e2e_pipelined(g, surf, stream, Vh, Uh, Wm, K), device="cuda")
-            e2e["serial_value"] = e2e["value"]
-            e2e["value"] = round(R.whole_job_rate(wl.ncell * K, ems_p * 1e-3, world) / 1e6, 1)
-            e2e["copies"] = ("pipelined: step s+1's surface is uploaded and step s's forces are read back on a "
-                             "copy stream while step s runs (double-buffered device arrays); all K uploads and "
-                             "K read-backs are inside the timed region")
+            serial = e2e["value"]
+            piped = round(R.whole_job_rate(wl.ncell * K, ems_p * 1e-3, world) / 1e6, 1)
+            # both loops keep every upload and read-back inside their timed
+            # region; the line reports the faster and lists both
+            e2e["serial_value"] = serial
+            e2e["pipelined_value"] = piped
+            e2e["value"] = max(serial, piped)
+            e2e["copies"] = ("the faster of two loops: serial (each step's uploads, step and read-back in order on one "
+                             "stream) and pipelined (step s+1's surface uploaded and step s's forces read back on a "
+                             "copy stream while step s runs, double-buffered device arrays); all K uploads and K "
+                             "read-backs are inside either timed region")
             e2e["note"] = ("the device-timed value records per-stage CUDA events in its timed region (for the "
                            "roofline's kernel time); these end-to-end loops record none, so they can come out "
                            "a few percent above it")
