@@ -58,7 +58,13 @@ template <auto KERNEL> static int resident_grid(int threads)
 // pairs whose link segment clearly misses: the plane is not reached (t = s1 / a
 // outside [0, 1] by more than a margin of 2e-3 cells, tested as s1 sign(a)
 // against [-margin, |a| + margin]) or the plane point lies outside the
-// triangle by more than 1% in barycentric terms.  Every remaining pair gets
+// triangle by more than 1% in barycentric terms.  The barycentric test is
+// used only where its own rounding is far below that margin: the plane
+// point carries an absolute error of a few float ulps of the coordinates
+// (about 2.4e-7 x the largest grid extent in cells x cl), and a barycentric
+// coordinate divides it by (shortest edge x sin^2 of the angle between the
+// edges), so triangles with a tiny edge or angle (slivers, nearly
+// coincident vertices) skip it and the exact test decides.  Every remaining pair gets
 // the exact, explicitly rounded test, so the link set does not depend on
 // this enumeration (the table keeps the minimum key per cell and direction).
 // Only a few lanes of a cell pass the prefilter, so the surviving pairs are
@@ -89,6 +95,9 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
         }
         const geom::TriPre tr = geom::tri_pre(s.V, ia, ib, ic);
         const float inv_den = __fdividef(1.0f, tr.den);
+        const float coord_err = 2.4e-7f * (float)max(g.nx, max(g.ny, g.nz)) * cl;
+        const bool bary_ok =
+            sqrtf(fminf(tr.d00, tr.d11)) * (tr.den / (tr.d00 * tr.d11)) > 400.0f * coord_err; // error < 0.0025
         float bmin[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
         float bmax[3] = {1.175494351e-38f, 1.175494351e-38f, 1.175494351e-38f};
         const uint32_t vid[3] = {ia, ib, ic};
@@ -150,7 +159,7 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
                     if (reach) {
                         const float sa = sg * s1;
                         cand = !(sa < -margin || sa > fa + margin);
-                        if (cand) {
+                        if (cand && bary_ok) {
                             // plane point relative to v0: p1 - t c cl - v0
                             const float t = s1 * inv_a;
                             const float wx = px - t * ccx, wy = py - t * ccy, wz = pz - t * ccz;
