@@ -132,6 +132,15 @@ def test_d3q27_walls_on_both_sides_of_the_wrap(cuda):
     check3(run_three(wl, 8))
 
 
+def test_d3q27_random_node_types(cuda):
+    """Walls, static solids and moving-solid cells scattered through an odd-
+    sized box and over its faces, an inlet and an outlet, random equilibrium
+    states: the product and the oracle against the reference's own step."""
+    from test_gpu_random_flags import _workload_3d
+
+    check3(run_three(_workload_3d(37, 21, 19, False, seed=5), 8))
+
+
 def test_d3q27_full_size_swimmer(cuda):
     """Config D at its full size (384 x 192 x 192, 4034-vertex undulating
     ellipsoid), 20 steps, product against the reference (the oracle is
