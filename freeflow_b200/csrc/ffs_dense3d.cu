@@ -375,6 +375,15 @@ __device__ __forceinline__ void wall_fix_part(const float *buf, int c_own, uint3
     }
 }
 
+// The planes of the ten moments, src + k ncell and dst + k ncell, as kernel
+// parameters: they sit in the constant bank, so a moment access of the 32-bit
+// index path forms its address from the cell index in one multiply-add
+// instead of adding k ncell first.
+template <typename T> struct MomentPlanes {
+    const T *src[10];
+    T *dst[10];
+};
+
 // ------------------------------------------------ staged moments (variant 3)
 // The moments of each halo plane come into shared memory by one TMA tiled
 // copy (cp.async.bulk.tensor, no multicast) two planes ahead, into one of two
@@ -448,7 +457,7 @@ constexpr uint32_t kStageWaitPolls = 1u << 22;
 // loads its halo cells' moments one plane ahead into registers.
 template <typename T, int MINB, bool IDX32, bool PAIRED, bool STAGE>
 __global__ void __launch_bounds__(D3::kThreads, MINB)
-    dense3d_kernel(GridArgs<T> g, int zchunk, const __grid_constant__ CUtensorMap tmap)
+    dense3d_kernel(GridArgs<T> g, const MomentPlanes<T> mp, int zchunk, const __grid_constant__ CUtensorMap tmap)
 {
     static_assert(!STAGE || (IDX32 && PAIRED), "staging is built for the paired 32-bit-index kernel");
     extern __shared__ __align__(128) float smem[];
@@ -519,8 +528,8 @@ __global__ void __launch_bounds__(D3::kThreads, MINB)
             const uint32_t io = zo + off_own, ir = zo + off_ring;
 #pragma unroll
             for (int k = 0; k < 10; ++k) {
-                mA[k] = g.src[io + (uint32_t)k * g.ncell];
-                if (has_ring) mB[k] = g.src[ir + (uint32_t)k * g.ncell];
+                mA[k] = mp.src[k][io];
+                if (has_ring) mB[k] = mp.src[k][ir];
             }
             hA = g.flags[io] & kTypeMask;
             if (has_ring) hB = g.flags[ir] & kTypeMask;
@@ -636,7 +645,7 @@ __global__ void __launch_bounds__(D3::kThreads, MINB)
         if (direct) {
             const uint32_t io = (uint32_t)halo_index(q, g.nz, wz) * (uint32_t)nxy + off;
 #pragma unroll
-            for (int k = 0; k < 10; ++k) raw[k] = g.src[io + (uint32_t)k * g.ncell];
+            for (int k = 0; k < 10; ++k) raw[k] = mp.src[k][io];
         } else {
             const T *st = stage_mem + (size_t)((q - zb + 1) & 1) * SG::kElems;
             const int e = (c / kHX) * SG::kBX + c % kHX + SG::kOff;
@@ -713,7 +722,7 @@ __global__ void __launch_bounds__(D3::kThreads, MINB)
                     const uint32_t idx = (uint32_t)(d * nxy + col);
                     float m[10];
                     collide3(R, g.omega, m);
-                    if constexpr (IDX32) encode_store_idx32<3, T>(m, g.dst, idx, g.ncell, g.codec);
+                    if constexpr (IDX32) encode_store<3, T>(m, mp.dst, idx, g.codec);
                     else encode_store_strided<3, T>(m, g.dst, (size_t)idx, g.ncell, g.codec);
                     if (bad_state<3>(m)) atomicOr(g.status, kStatusNonFinite);
                     if (fp & kBitOutletSrc) {
@@ -735,9 +744,11 @@ __global__ void __launch_bounds__(D3::kThreads, MINB)
                 for (int k = 0; k < 6; ++k) f2split(Sp[k], lo[k], hi[k]);
                 slice_add<-1>(Rp, lo);
                 slice_add<0>(Rc, Sm);
-                if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
-                if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
-                if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                if ((wc | wp) & kWall) { // near-wall cells only: one test on the common path
+                    if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
+                    if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
+                    if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                }
                 float R[10];
                 raw_from_scaled(Rp, R);
                 // Rp is free: it becomes the cell at z = p + 1
@@ -750,9 +761,11 @@ __global__ void __launch_bounds__(D3::kThreads, MINB)
                 slice_add<-1>(Rp, S);
                 slice_sums(buf, 1, c_own, S);
                 slice_add<0>(Rc, S);
-                if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
-                if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
-                if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                if ((wc | wp) & kWall) {
+                    if (wc & kWall) add_reflected<PAIRED>(buf, c_own, wc & kWall, Rc);
+                    if (wp & kWall & oor_p) wall_fix_part<PAIRED>(buf, c_own, wp & kWall & oor_p, 0, Rp);
+                    if (wc & kWall & oor_xy) wall_fix_part<PAIRED>(buf, c_own, wc & kWall & oor_xy, 1, Rc);
+                }
                 {
                     float R[10];
                     raw_from_scaled(Rp, R);
@@ -902,7 +915,12 @@ template <typename T, int MINB, bool IDX32, bool PAIRED, bool STAGE> struct Dens
         int nchunk = choose_zchunks(tx * ty, g.nz, slots);
         int zchunk = (g.nz + nchunk - 1) / nchunk;
         dim3 grid(tx, ty, (g.nz + zchunk - 1) / zchunk);
-        dense3d_kernel<T, MINB, IDX32, PAIRED, STAGE><<<grid, D3::kThreads, smem, s>>>(g, zchunk, map);
+        MomentPlanes<T> mp;
+        for (int k = 0; k < 10; ++k) {
+            mp.src[k] = g.src + (size_t)k * g.ncell;
+            mp.dst[k] = g.dst + (size_t)k * g.ncell;
+        }
+        dense3d_kernel<T, MINB, IDX32, PAIRED, STAGE><<<grid, D3::kThreads, smem, s>>>(g, mp, zchunk, map);
         return cudaGetLastError();
     }
 };
