@@ -60,8 +60,8 @@ FALLBACK_HBM_GBS = 6650.0
 # (dram__bytes_read.sum + dram__bytes_write.sum), scaled to a launch by the
 # cells it processes; the capture and its command are in the named profile.
 DENSE_TRAFFIC_PER_CELL = {
-    (3, "f32"): (75.55, "profiles/dense3d_link_kernels_D3Q27_256x128x128_swimmer_f32.md"),
-    (3, "f16"): (35.72, "profiles/dense3d_D3Q27_256x128x128_swimmer_f16.md"),
+    (3, "f32"): (75.20, "profiles/dense3d_link_kernels_D3Q27_256x128x128_swimmer_f32.md"),
+    (3, "f16"): (35.98, "profiles/dense3d_D3Q27_256x128x128_swimmer_f16.md"),
 }
 
 

@@ -968,7 +968,10 @@ cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant)
 }
 
 // Times each variant on this grid (the pass only reads src and writes dst, so
-// repeating it is harmless) and returns the faster one.
+// repeating it is harmless) and returns the fastest.  Variant 2 is timed
+// first and kept unless another is at least 1 % faster: all give the same
+// bits, so the margin only keeps the choice stable, and on B200 variant 2 is
+// the fastest for FP32 and FP16 storage.
 template <typename T>
 int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
 {
@@ -981,25 +984,22 @@ int tune_dense3d(const GridArgs<T> &g, cudaStream_t s)
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     float best = 1e30f;
-    int best_v = 0;
-    // the scalar layout for two and three CTAs per SM and the paired layout,
-    // which all round identically
-    for (int v = 0; v < kDense3dVariants; ++v) {
+    int best_v = -1;
+    constexpr int kOrder[kDense3dVariants] = {2, 0, 1, 3};
+    for (int v : kOrder) {
         if (!dense3d_has_variant<T>(v, g)) continue;
         if (launch_dense3d<T>(g, s, v) != cudaSuccess) continue; // warm-up
         cudaEventRecord(a, s);
-        for (int r = 0; r < 3; ++r) launch_dense3d<T>(g, s, v);
+        for (int r = 0; r < 5; ++r) launch_dense3d<T>(g, s, v);
         cudaEventRecord(b, s);
         cudaEventSynchronize(b);
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, a, b);
-        // a later variant must win clearly (both give the same bits; this
-        // only keeps the choice stable)
-        if (ms < (v == 0 ? 1.0f : 0.97f) * best) { best = ms; best_v = v; }
+        if (best_v < 0 || ms < 0.99f * best) { best = ms; best_v = v; }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    return best_v;
+    return best_v < 0 ? 0 : best_v;
 }
 
 template cudaError_t launch_dense3d<float>(const GridArgs<float> &, cudaStream_t, int);
