@@ -248,8 +248,14 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
     uint32_t hit_elem = 0xffffffffu;
     uint32_t vshare[3] = {0, 0, 0};
     float share[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; // [vertex][component]
+    // Every load the update may need goes out before any of them is tested:
+    // the cell's own moments and, per lane, the node type of the wrapped
+    // neighbour, the link key and the moments of the cell an ordinary pull
+    // reads (a lane that takes the bounce-back or a moving-wall link discards
+    // its pull).  The update then waits for one round of loads where testing
+    // the node type and the key first would make it wait for three.
+    load_moments<DIM, T>(mc, g.src, g.ncell, cell, g.codec);
     if (upd) {
-        load_moments<DIM, T>(mc, g.src, g.ncell, cell, g.codec);
         Coef<DIM> own;
         own.make(mc);
         if (lane < Q) {
@@ -261,17 +267,31 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
             // the wrapped neighbour (x1, y1, z1 are within one cell of the grid)
             auto wrap1 = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
             const uint32_t ib = (uint32_t)wrap1(z1, g.nz) * nxy + (uint32_t)wrap1(y1, g.ny) * nx + (uint32_t)wrap1(x1, g.nx);
+            // the ordinary pull's source: the upstream halo cell (halo_index)
+            const int sx = halo_index(x1, g.nx, wx), sy = halo_index(y1, g.ny, wy), sz = halo_index(z1, g.nz, wz);
+            const uint32_t sidx = (uint32_t)sz * nxy + (uint32_t)sy * nx + (uint32_t)sx;
+            const uint8_t fb = g.flags[ib];
+            const unsigned long long key = notCross ? links[(size_t)slot * Q + i] : ~0ull;
+            float pulled;
+            {
+                float mn[NM];
+                load_moments<DIM, T>(mn, g.src, g.ncell, sidx, g.codec);
+                Coef<DIM> nc;
+                nc.make(mn);
+                float v = nc.population(cx, cy, cz);
+                if (HALF) v = round_half(v);
+                pulled = fmaxf(v, 0.0f);
+            }
             bool done = false;
             // a wall neighbour: bounce-back, no link (with wall_stream in 2D, the
             // reference's 2D kernel: the ordinary pull, no link either)
-            const bool bb = is_bounce_back<DIM>(g.flags[ib] & kTypeMask);
+            const bool bb = is_bounce_back<DIM>(fb & kTypeMask);
             if (bb && !(DIM == 2 && g.wall_stream)) {
                 float v = own.population(-cx, -cy, -cz);
                 if (HALF) v = round_half(v);
                 pop = fmaxf(v, 0.0f);
                 done = true;
             } else if (!bb && notCross) {
-                const unsigned long long key = links[(size_t)slot * Q + i];
                 if (key != ~0ull) {
                     const uint32_t e = (uint32_t)(key & 0xffffffffull);
                     const float cl = sc.cl;
@@ -329,18 +349,7 @@ __device__ __forceinline__ void link_cell_update(const GridArgs<T> &g, const uns
                     }
                 }
             }
-            if (!done) {
-                // ordinary pull from the upstream halo cell (halo_index)
-                const int sx = halo_index(x1, g.nx, wx), sy = halo_index(y1, g.ny, wy), sz = halo_index(z1, g.nz, wz);
-                const uint32_t sidx = (uint32_t)sz * nxy + (uint32_t)sy * nx + (uint32_t)sx;
-                float mn[NM];
-                load_moments<DIM, T>(mn, g.src, g.ncell, sidx, g.codec);
-                Coef<DIM> nc;
-                nc.make(mn);
-                float v = nc.population(cx, cy, cz);
-                if (HALF) v = round_half(v);
-                pop = fmaxf(v, 0.0f);
-            }
+            if (!done) pop = pulled;
         }
     }
     // forces: one share per (link, element vertex), summed per element
