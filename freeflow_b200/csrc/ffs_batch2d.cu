@@ -192,10 +192,13 @@ __global__ void __launch_bounds__(TX, 1024 / TX) pool_strip_kernel(const PoolEpi
         // kPer cells (then so does every moment plane; the buffers themselves
         // are 256-byte aligned)
         const bool vec = g.nx % kPer == 0;
-        // stage row r (yb-1 <= r <= ye): the cells that lie inside the grid
-        auto issue = [&](int r) {
+        // staging slot of row r (r >= -1): (r + 1) mod kStage, kept as a
+        // counter in the row loop below instead of a division per row
+        auto slot_of = [](int r) { return (uint32_t)(r + 1) % (uint32_t)kStage; };
+        // stage row r (yb-1 <= r <= ye) into slot sl: the cells that lie inside the grid
+        auto issue = [&](int r, uint32_t sl) {
             if (r <= ye) {
-                T (*st)[kSW] = stage[(r + kStage) % kStage];
+                T (*st)[kSW] = stage[sl];
                 const uint32_t row = (uint32_t)halo_index(r, g.ny, wy) * (uint32_t)g.nx;
                 if (vec) {
                     for (int e = tid; e < 6 * kCopies; e += TX) {
@@ -216,12 +219,12 @@ __global__ void __launch_bounds__(TX, 1024 / TX) pool_strip_kernel(const PoolEpi
         // reconstruct this thread's halo cell x0-1+tid of row r into the
         // ring; the clamped or wrapped source column is read from the staged
         // row when it lies there, else (a wrapped edge) from memory
-        auto recon = [&](int r) {
+        auto recon = [&](int r, uint32_t sl) {
             const int gx = halo_index(x0 - 1 + tid, g.nx, wx);
             const int j = gx - xs;
             T raw[6];
             if (j >= 0 && j < kSW) {
-                const T (*st)[kSW] = stage[(r + kStage) % kStage];
+                const T (*st)[kSW] = stage[sl];
 #pragma unroll
                 for (int k = 0; k < 6; ++k) raw[k] = st[k][j];
             } else {
@@ -231,13 +234,13 @@ __global__ void __launch_bounds__(TX, 1024 / TX) pool_strip_kernel(const PoolEpi
             }
             float f[9];
             dense2d_recon<T, false>(g, raw, f);
-            float (*rg)[TX] = ring[(r + kRing) % kRing];
+            float (*rg)[TX] = ring[(uint32_t)(r + kRing) % kRing];
 #pragma unroll
             for (int i = 0; i < 9; ++i) rg[i][tid] = f[i];
         };
 
 #pragma unroll
-        for (int r = 0; r < kDepth; ++r) issue(yb - 1 + r);
+        for (int r = 0; r < kDepth; ++r) issue(yb - 1 + r, slot_of(yb - 1 + r));
         const int x = x0 - 1 + tid;
         const bool owner = tid >= 1 && tid <= kOut && x < g.nx; // this thread updates column x
         // flag bytes of this thread's cell: at the top of iteration r, f8 is
@@ -247,18 +250,22 @@ __global__ void __launch_bounds__(TX, 1024 / TX) pool_strip_kernel(const PoolEpi
             return (owner && y >= yb && y < ye) ? (uint32_t)g.flags[(uint32_t)y * (uint32_t)g.nx + (uint32_t)x] : 0u;
         };
         uint32_t f8 = 0, f8n = 0;
+        uint32_t sl = slot_of(yb - 1);                  // slot of row r
+        uint32_t sl_prev = sl == 0 ? kStage - 1 : sl - 1; // slot of row r-1 = slot of row r + kDepth
         for (int r = yb - 1; r <= ye + 1; ++r) {
             cp_async_wait<kDepth - 1>(); // this thread's copies of row r have landed
             __syncthreads();             // everyone's copies of row r, and ring row r-1, are visible
-            issue(r + kDepth);           // into the slot of row r-1, reconstructed last iteration
-            if (r <= ye) recon(r);
+            issue(r + kDepth, sl_prev);  // into the slot of row r-1, reconstructed last iteration
+            if (r <= ye) recon(r, sl);
+            sl_prev = sl;
+            sl = sl + 1 == kStage ? 0u : sl + 1;
             // output row o: its ring rows o-1, o, o+1 were written before the barrier
             const int o = r - 2;
             if (o >= yb && owner && is_updated(f8 & kTypeMask) && !(f8 & kBitLink)) {
                 const uint32_t idx = (uint32_t)(o * g.nx + x);
                 dense2d_update_cell<T, true>(
-                    g, idx, f8, [&](int i) { return ring[(o - L::cy(i) + kRing) % kRing][i][tid - L::cx(i)]; },
-                    [&](int i) { return ring[(o + kRing) % kRing][i][tid]; });
+                    g, idx, f8, [&](int i) { return ring[(uint32_t)(o - L::cy(i) + kRing) % kRing][i][tid - L::cx(i)]; },
+                    [&](int i) { return ring[(uint32_t)(o + kRing) % kRing][i][tid]; });
             }
             f8 = f8n;
             f8n = flag_at(o + 2);
