@@ -122,6 +122,13 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
         const bool reach = fa > margin;              // else: the link runs (nearly) parallel to the plane
         const float sg = a > 0.0f ? 1.0f : -1.0f;
         const float inv_a = reach ? __fdividef(1.0f, a) : 0.0f;
+        // the largest plane distance |s1| that any lane's test below accepts
+        // (fa + margin, or 2 margin for a lane parallel to the plane): a cell
+        // farther from the plane has no candidate, and the whole warp skips
+        // it (s1 is the same for every lane)
+        float reach_max = act ? (reach ? fa + margin : 2.0f * margin) : 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) reach_max = fmaxf(reach_max, __shfl_xor_sync(full, reach_max, o));
         // the exact test of cell (i, j, k3), direction ll, and the insertion on a hit
         auto exact = [&](int i, int j, int k3, int ll) {
             int dx, dy, dz;
@@ -155,6 +162,7 @@ __global__ void __launch_bounds__(256) detect_links3_kernel(GridArgs<T> g, uint3
                 for (int i = lo[0]; i <= hi[0]; ++i) {
                     const float px = (float)i * cl - tr.v0[0];
                     const float s1 = fmaf(tr.n[0], px, s_yz);
+                    if (fabsf(s1) > reach_max) continue;
                     bool cand;
                     if (reach) {
                         const float sa = sg * s1;
