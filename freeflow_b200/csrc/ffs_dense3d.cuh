@@ -20,8 +20,8 @@ static_assert(D3::kRing <= D3::kThreads, "every ring cell needs a partner thread
 // two planes ahead (grids whose rows of moments are not a multiple of 16
 // bytes run 2; on 384 x 192 x 192 it ran 5 % slower than 2, so the tuner
 // keeps 2 there).  All
-// round identically; the first step times them and keeps the fastest
-// (FFS_DENSE3D_VARIANT pins one).
+// round identically; the first step times them, variant 2 first, and keeps
+// another only if it is at least 1 % faster (FFS_DENSE3D_VARIANT pins one).
 constexpr int kDense3dVariants = 4;
 template <typename T> cudaError_t launch_dense3d(const GridArgs<T> &g, cudaStream_t s, int variant);
 template <typename T> int tune_dense3d(const GridArgs<T> &g, cudaStream_t s);
